@@ -1,0 +1,356 @@
+#!/usr/bin/env python
+"""Benchmark of the split-step spinor propagator on B200.
+
+Workload (the q2D configuration the headline metric is quoted on): spin-2
+SO-coupled real-time dynamics, NX=NY=512, DX=DY=0.05, DT=1e-4, Rb-87
+(mass 87, a0/a2/a4 = 87.93/91.28/99.18 a_B), NATOMS=50000, NUX=NUY=20 Hz,
+NUZ=500 Hz, ground state at GAMMAX=GAMMAY=1.0 quenched to GAMMAX=1.2.
+Synthetic initial state: the reference's default Gaussian guess relaxed by
+imaginary-time steps at gamma=(1,1) on the device, plus 1e-3 complex Gaussian
+noise (numpy PCG64 seed 2), renormalised (no dataset is involved).
+
+A step is one full Lie split step FFT->KE->SOC->BFT->SE->SP->NORMC of the
+whole 512^2 x 5 spinor.  Metric: grid-pt*steps/s (higher is better).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--precision fp64|fp32]
+
+value : device time (CUDA events on the launching stream) of K steps, L2
+        flushed (256 MiB write) before every step, max over ranks.
+e2e   : the same K steps through the C ABI with host buffers: pinned H2D of
+        the state, every step's NORMC read back asynchronously to pinned
+        memory, D2H of the final state; device-timed with the same flushes.
+The reference arm (--impl reference) times the CPU restatement of the
+reference (oracle/, OpenMP on all host cores) on the same workload: the
+Fortran/FFTW/LAPACK reference cannot be compiled on this image.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = dict(name="q2d-spin2-SO-realtime-512x512-quench", dim=2, spin=2, n=(512, 512),
+                d=(0.05, 0.05), dt=1e-4, mass=87.0, a=(87.93, 91.28, 99.18), natoms=50000,
+                nu=(20.0, 20.0, 500.0), gamma_gs=(1.0, 1.0), gamma=(1.2, 1.0))
+METRIC = "grid-pt*steps/s"
+
+
+def workload_config(gamma):
+    from fortress_b200.config import RunConfig
+    w = WORKLOAD
+    c = RunConfig(dim=2, spin=2, n=(512, 512, 1), d=(0.05, 0.05, 1.0), dt=w["dt"], mass=w["mass"],
+                  a=w["a"], natoms=w["natoms"], nu=w["nu"], switch_im=0,
+                  gamma=(gamma[0], gamma[1], 0.0))
+    return c
+
+
+def gaussian_guess(cfg):
+    """INITIALIZE default spin-2 guess, cgpe2d.f90:766-771."""
+    import numpy as np
+    nx, ny = cfg.n[0], cfg.n[1]
+    x = (-1.0 + 2.0 * np.arange(nx) / nx) * nx * cfg.d[0] / 2.0
+    y = (-1.0 + 2.0 * np.arange(ny) / ny) * ny * cfg.d[1] / 2.0
+    ax, ay, _ = cfg.alpha
+    g = np.sqrt(0.2) * np.exp(-(ax * x[:, None] ** 2 + ay * y[None, :] ** 2) / 2.0) / np.sqrt(np.pi)
+    return np.repeat(g[:, :, None], 5, axis=2).astype(np.complex128)
+
+
+def add_noise(phi, seed=2):
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    phi = phi + 1e-3 * (rng.standard_normal(phi.shape) + 1j * rng.standard_normal(phi.shape)) * np.abs(phi).max()
+    return phi
+
+
+def prepared_state(F, cfg_gs, prep_steps=3000):
+    """Ground-state-like start: imaginary time on the device from the guess."""
+    import numpy as np
+    p = cfg_gs.params()
+    p["imag_time"] = True
+    p["dt"] = 1e-3
+    prop = F.Propagator(**p)
+    prop.set_state(gaussian_guess(cfg_gs))
+    prop.normt()
+    prop.step(prep_steps)
+    phi = add_noise(prop.state().reshape(512, 512, 5))
+    prop.close()
+    # renormalise to the Simpson norm 1 (NORMT of the reference)
+    from fortress_b200.config import simpson_weights
+    w = simpson_weights(512, cfg_gs.d[0])
+    tot = float(np.einsum("i,j,ijm->", w, w, np.abs(phi) ** 2))
+    return phi / np.sqrt(tot)
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index=0):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{index}.csv")
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, smax, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1])); smax = max(smax, float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def known_traffic(workload, precision, kernel):
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return d.get(f"{workload}/{precision}/{kernel}")
+    except Exception:
+        return None
+
+
+# --------------------------------------------------------------- CPU legs
+def run_cpu(phi, cfg, steps, warmup, budget_s=None):
+    from oracle import oracle as O
+    t = cfg.tau()
+    orc = O.Oracle(dim=2, spin=2, nx=512, ny=512, dx=cfg.d[0], dy=cfg.d[1], dt=cfg.dt, imag=0, tau=t,
+                   gx=cfg.gamma[0], gy=cfg.gamma[1], ax=cfg.alpha[0], ay=cfg.alpha[1], az=cfg.alpha[2])
+    orc.set_state(phi)
+    for _ in range(warmup):
+        orc.step(1)
+    done, t0 = 0, time.perf_counter()
+    while done < steps:
+        orc.step(1)
+        done += 1
+        if budget_s is not None and time.perf_counter() - t0 > budget_s and done >= 2:
+            break
+    el = time.perf_counter() - t0
+    return 512 * 512 * done / el, done, el, O.num_threads()
+
+
+# -------------------------------------------------------------------- main
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        return reference_arm(args, rank, world)
+
+    import numpy as np
+    import torch
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+    import fortress_b200 as F
+
+    cfg_gs = workload_config(WORKLOAD["gamma_gs"])
+    cfg = workload_config(WORKLOAD["gamma"])
+    phi0 = prepared_state(F, cfg_gs)
+
+    prop = F.Propagator(**cfg.params(args.precision))
+    stream = torch.cuda.current_stream()
+    prop.set_stream(stream.cuda_stream)
+    prop.set_state(phi0)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    npts = 512 * 512
+    ms_comp, cs = 5, (16 if args.precision == "fp64" else 8)
+
+    for _ in range(args.warmup):
+        flush.zero_()
+        prop.step(1, snapshot=False)
+    torch.cuda.synchronize()
+
+    # ---------------------------------------------------------- value
+    prop.profile(True)
+    prop.profile_read(reset=True)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = prop.kernel_launches()
+    for k in range(args.steps):
+        flush.zero_()
+        evs[k][0].record(stream)
+        prop.step(1, snapshot=False)
+        evs[k][1].record(stream)
+    torch.cuda.synchronize()
+    launches = prop.kernel_launches() - l0
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    total_ms = sum(a.elapsed_time(b) for a, b in evs)
+    kms, kn = prop.profile_read(reset=True)
+    prop.profile(False)
+    t_max = total_ms
+    if dist:
+        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+    value = world * npts * args.steps / (t_max / 1e3)
+
+    # --------------------------------------------------- e2e (host buffers)
+    phi_host = torch.empty(npts * ms_comp * 2, dtype=torch.float64, pin_memory=True)
+    phi_host.numpy()[:] = np.ascontiguousarray(phi0.reshape(-1, order="F")).view(np.float64)
+    out_host = torch.empty_like(phi_host).pin_memory()
+    norms_host = torch.empty(args.steps * ms_comp, dtype=torch.float64, pin_memory=True)
+    e2e_ms = 0.0
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * args.steps + 4)]
+    flush.zero_()
+    ev[0].record(stream)
+    prop.set_state_host_ptr(phi_host.data_ptr())
+    ev[1].record(stream)
+    for k in range(args.steps):
+        if k:
+            flush.zero_()
+        ev[2 + 2 * k].record(stream)
+        prop.step(1, snapshot=(k == args.steps - 1))
+        prop.norms_async(norms_host.data_ptr() + 8 * ms_comp * k)
+        ev[3 + 2 * k].record(stream)
+    flush.zero_()
+    ev[2 * args.steps + 2].record(stream)
+    prop.get_state_host_ptr(out_host.data_ptr())
+    ev[2 * args.steps + 3].record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = ev[0].elapsed_time(ev[1]) + ev[2 * args.steps + 2].elapsed_time(ev[2 * args.steps + 3])
+    e2e_ms += sum(ev[2 + 2 * k].elapsed_time(ev[3 + 2 * k]) for k in range(args.steps))
+    norms = norms_host.numpy().reshape(args.steps, ms_comp)
+    assert np.all(np.isfinite(norms)) and abs(norms[-1].sum() - norms[0].sum()) < 1e-6 * norms[0].sum()
+    if dist:
+        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * npts * args.steps / (e2e_ms / 1e3)
+    state_bytes = npts * ms_comp * 16
+
+    # ------------------------------------------------------------ roofline
+    classes = ["row_x", "col_y", "col_z", "oned"]
+    dom = int(np.argmax(kms))
+    per_launch_ms = kms[dom] / max(kn[dom], 1)
+    alg_bytes = 2 * ms_comp * npts * cs               # read + write of the spinor
+    peak, peak_kind = measured_peaks()
+    achieved = alg_bytes / (per_launch_ms / 1e3) / 1e9
+    kernels = {classes[i]: {"launches": int(kn[i]), "ms_per_launch": float(kms[i] / kn[i]),
+                            "share": float(kms[i] / kms.sum())} for i in range(4) if kn[i]}
+
+    result = {
+        "metric": METRIC, "value": value, "unit": "grid-pt*steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "c128" if args.precision == "fp64" else "c64",
+        "data": "synthetic (relaxed Gaussian guess + seeded noise)",
+        "config": {"workload": WORKLOAD["name"], "grid": [512, 512], "spin": 2, "components": 5,
+                   "time": "real", "dt": WORKLOAD["dt"], "precision": args.precision,
+                   "parallelism": f"replicas{world}" if world > 1 else "single",
+                   "l2": "flushed before every timed step (256 MiB write)"},
+        "e2e": {"value": e2e_value, "unit": "grid-pt*steps/s",
+                "h2d_bytes_per_step": state_bytes / args.steps,
+                "d2h_bytes_per_step": 8 * ms_comp + state_bytes / args.steps},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "kernel": classes[dom], "achieved": achieved, "peak": peak,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": known_traffic(WORKLOAD["name"], args.precision, classes[dom]),
+                     "alg_bytes_per_launch": alg_bytes},
+        "kernels": kernels,
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, done, el, thr = run_cpu(phi0, cfg, steps=30, warmup=1, budget_s=12.0)
+        result["cpu_baseline"] = {"value": rate, "unit": "grid-pt*steps/s", "cores": thr, "kind": "port",
+                                  "sample": f"{done} steps of the same 512^2 workload ({el:.1f} s, oracle/ FP64 OpenMP)"}
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(result))
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return 0
+    import numpy as np  # noqa: F401
+    cfg = workload_config(WORKLOAD["gamma"])
+    phi = add_noise(gaussian_guess(cfg))
+    rate, done, el, thr = run_cpu(phi, cfg, steps=args.steps, warmup=args.warmup, budget_s=90.0)
+    res = {"metric": METRIC, "value": rate, "unit": "grid-pt*steps/s", "n_gpus": world, "steps": done,
+           "warmup": args.warmup, "ms_per_step": 1e3 * el / done, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "c128", "impl": "reference",
+           "data": "synthetic (Gaussian guess + seeded noise)",
+           "config": {"workload": WORKLOAD["name"], "grid": [512, 512], "spin": 2, "time": "real",
+                      "precision": "fp64", "parallelism": "cpu"},
+           "cpu_baseline": {"value": rate, "unit": "grid-pt*steps/s", "cores": thr, "kind": "port",
+                            "sample": f"{done} timed steps after {args.warmup} warm-up steps"},
+           "e2e": {"value": rate, "unit": "grid-pt*steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(res))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main() or 0)

@@ -1,0 +1,833 @@
+// fgpe_api.cu -- host side of the C ABI declared in include/fgpe.h.
+//
+// A handle owns every device buffer of one propagator instance:
+//   S     x-spectral spinor (2D/3D), complex T, PHI layout (NX,NY,NZ,M)
+//   psi   real-space spinor (the current state is info[SCALE] * psi)
+//   prev  real-space spinor one step older (for CONV)
+//   tables: k grids, x grids, Simpson weights, trap parts, twiddles, KE factors
+// Launch shapes (rows per block, column tile widths, threads) are chosen once
+// at creation from the grid size and the shared-memory budget.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "../../include/fgpe.h"
+#include "fgpe_kernels.cuh"
+
+using namespace fgpe;
+
+namespace {
+
+const double kPi = 3.14159265358979323846264338327950288;
+thread_local std::string g_last_error;
+
+struct Launch {
+    int T = 0;
+    size_t smem = 0;
+    int tile = 0;          // rows (row pass) or TX (column pass)
+    dim3 grid;
+};
+
+}  // namespace
+
+struct fgpe_s {
+    fgpe_params p;
+    int ms = 0;
+    long long npts = 0;
+    int fp32 = 0;
+    size_t cs = 16;        // bytes per complex element in device buffers
+    cudaStream_t st = nullptr;
+    bool own_stream = false;
+    StepConst sc;
+    void *S = nullptr, *psi = nullptr, *prev = nullptr, *stage = nullptr;
+    double *info = nullptr, *info_prev = nullptr, *obs = nullptr, *part = nullptr;
+    unsigned* counters = nullptr;
+    int* pmap = nullptr;         // position->frequency maps of the three axes
+    double* dtab = nullptr;
+    void* ctab = nullptr;
+    double* h_small = nullptr;   // pinned, 64 doubles
+    Launch row, col[3], k1, obsl;
+    bool psi_valid = false, S_valid = false, prev_valid = false, norms_valid = false, has_state = false;
+    long long launches = 0;
+    std::string msg;
+    // kernel timing (fgpe_profile_enable)
+    bool prof = false;
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<std::pair<int, int>> ev_rec;   // (class, pool index of start)
+    double prof_ms[4] = {0, 0, 0, 0};
+    long long prof_n[4] = {0, 0, 0, 0};
+};
+
+namespace {
+
+int fail(fgpe_t* h, int code, const std::string& m) {
+    if (h) h->msg = m;
+    g_last_error = m;
+    return code;
+}
+
+#define CK(call)                                                                          \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return fail(h, FGPE_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+bool plan_fft(int n, FftPlan* pl) {
+    pl->n = n; pl->nf = 0;
+    int m = n;
+    std::vector<int> f;
+    while (m % 8 == 0) { f.push_back(8); m /= 8; }
+    if (m % 4 == 0) { f.push_back(4); m /= 4; }
+    if (m % 2 == 0) { f.push_back(2); m /= 2; }
+    while (m % 3 == 0) { f.push_back(3); m /= 3; }
+    while (m % 5 == 0) { f.push_back(5); m /= 5; }
+    if (m != 1 || f.size() > 16) return false;
+    for (size_t i = 0; i < f.size(); ++i) pl->r[i] = f[i];
+    pl->nf = (int)f.size();
+    return true;
+}
+
+// Largest per-thread load of a pass: nlines*n elements split so that each
+// thread keeps at most 16 complex values (15 for radix 3 and 5).
+int threads_needed(int nel, const FftPlan& pl) {
+    int need = 32;
+    for (int i = 0; i < pl.nf; ++i) {
+        const int R = pl.r[i];
+        const int K = 16 / R;
+        const int nb = nel / R;
+        need = std::max(need, (nb + K - 1) / K);
+    }
+    return need;
+}
+
+int round32(int x) { return (x + 31) / 32 * 32; }
+
+// simpson.f90:4-21 applied to unit vectors: the weight of every node.
+std::vector<double> simpson_weights(int n, double dx) {
+    std::vector<double> w(n, 0.0);
+    if (n == 1) { w[0] = 1.0; return w; }
+    std::vector<double> f(n, 0.0);
+    for (int t = 0; t < n; ++t) {
+        std::fill(f.begin(), f.end(), 0.0);
+        f[t] = 1.0;
+        double f1 = f[1] + f[n - 5], f2 = f[2];
+        for (int i = 4; i <= n - 6; i += 2) { f1 += f[i - 1]; f2 += f[i]; }
+        w[t] = dx * (f[0] + 4.0 * f1 + 2.0 * f2 + f[n - 4]) / 3.0 + 3.0 * dx * (f[n - 4] + 3.0 * (f[n - 3] + f[n - 2]) + f[n - 1]) / 8.0;
+    }
+    return w;
+}
+
+template <typename T, int MS> void set_smem_attrs() {
+    cudaFuncSetAttribute(k_row<T, MS>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    cudaFuncSetAttribute(k_col<T, MS>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    cudaFuncSetAttribute(k_1d<T, MS>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+}
+
+// Event pair around one launch when profiling is on.
+struct ProfScope {
+    fgpe_t* h; int cls; int idx = -1;
+    ProfScope(fgpe_t* hh, int c) : h(hh), cls(c) {
+        if (!h->prof) return;
+        idx = (int)h->ev_rec.size() * 2;
+        while ((int)h->ev_pool.size() < idx + 2) {
+            cudaEvent_t e; cudaEventCreate(&e); h->ev_pool.push_back(e);
+        }
+        cudaEventRecord(h->ev_pool[idx], h->st);
+    }
+    ~ProfScope() {
+        if (idx < 0) return;
+        cudaEventRecord(h->ev_pool[idx + 1], h->st);
+        h->ev_rec.push_back({cls, idx});
+    }
+};
+
+// ---------------------------------------------------------------- launches
+template <typename T, int MS>
+void launch_row(fgpe_t* h, int mode, void* snap) {
+    RowArgs a;
+    a.S = h->S; a.psi = h->psi; a.snap = snap; a.part = h->part; a.counter = h->counters;
+    a.info = h->info; a.rows = h->row.tile; a.mode = mode;
+    ProfScope ps(h, 0);
+    k_row<T, MS><<<h->row.grid, h->row.T, h->row.smem, h->st>>>(h->sc, a);
+    h->launches++;
+}
+
+template <typename T, int MS>
+void launch_col(fgpe_t* h, int axis, int flags) {
+    ColArgs a;
+    a.S = h->S;
+    a.tw = axis == 1 ? h->sc.twy : h->sc.twz;
+    a.plan = axis == 1 ? h->sc.py : h->sc.pz;
+    a.info = h->info;
+    a.cfac = 1.0 / (double)h->npts;
+    a.n = axis == 1 ? h->p.ny : h->p.nz;
+    a.axis_stride = axis == 1 ? h->p.nx : (long long)h->p.nx * h->p.ny;
+    a.other_stride = h->p.dim == 2 ? 0 : (axis == 1 ? (long long)h->p.nx * h->p.ny : h->p.nx);
+    a.tx = h->col[axis].tile;
+    a.flags = flags;
+    ProfScope ps(h, axis);
+    k_col<T, MS><<<h->col[axis].grid, h->col[axis].T, h->col[axis].smem, h->st>>>(h->sc, a);
+    h->launches++;
+}
+
+template <typename T, int MS>
+void launch_obs(fgpe_t* h, int mode, bool with_prev) {
+    ObsArgs a;
+    a.psi = h->psi; a.prev = with_prev ? h->prev : nullptr;
+    a.info = h->info; a.info_prev = h->info_prev;
+    a.part = h->part; a.counter = h->counters + 1; a.out = h->obs;
+    a.dx = h->p.dx; a.dy = h->p.dy; a.dz = h->p.dz; a.mode = mode;
+    k_obs<T, MS><<<h->obsl.grid, 256, 0, h->st>>>(h->sc, a);
+    h->launches++;
+}
+
+template <typename T, int MS>
+void launch_point(fgpe_t* h, int op, double factor) {
+    PointArgs a; a.psi = h->psi; a.op = op; a.factor = factor;
+    const long long blocks = std::min<long long>((h->npts + 255) / 256, 148LL * 16);
+    k_pointwise_op<T, MS><<<(unsigned)blocks, 256, 0, h->st>>>(h->sc, a);
+    h->launches++;
+}
+
+template <typename T, int MS>
+void launch_1d(fgpe_t* h, int nsteps, void* snap_prev) {
+    OneDArgs a;
+    a.psi = h->psi; a.snap_prev = snap_prev; a.info = h->info; a.info_prev = h->info_prev;
+    a.nsteps = nsteps;
+    ProfScope ps(h, 3);
+    k_1d<T, MS><<<1, h->k1.T, h->k1.smem, h->st>>>(h->sc, a);
+    h->launches++;
+}
+
+// dispatch on (precision, spin)
+#define DISPATCH(h, FN, ...)                                                  \
+    do {                                                                      \
+        if ((h)->fp32) {                                                      \
+            if ((h)->ms == 3) FN<float, 3>(__VA_ARGS__); else FN<float, 5>(__VA_ARGS__);   \
+        } else {                                                              \
+            if ((h)->ms == 3) FN<double, 3>(__VA_ARGS__); else FN<double, 5>(__VA_ARGS__); \
+        }                                                                     \
+    } while (0)
+
+template <typename T>
+__global__ void k_export(const T* psi, double* out, long long n2, const double* info) {
+    const double s = info[INFO_SCALE];
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n2; t += (long long)gridDim.x * blockDim.x)
+        out[t] = s * (double)psi[t];
+}
+template <typename T>
+__global__ void k_import(const double* in, T* psi, long long n2) {
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n2; t += (long long)gridDim.x * blockDim.x)
+        psi[t] = (T)in[t];
+}
+
+int check_err(fgpe_t* h) {
+    CK(cudaStreamSynchronize(h->st));
+    CK(cudaGetLastError());
+    return FGPE_OK;
+}
+
+// Digit-reversed position -> frequency index of the in-place DIF transform
+// with radices r[0..nf-1] (r[0] acts on the longest stride).
+std::vector<int> position_map(const FftPlan& pl) {
+    const int n = pl.n;
+    std::vector<int> f(n);
+    for (int k = 0; k < n; ++k) {
+        int rem = k, pos = 0, block = n;
+        for (int p = 0; p < pl.nf; ++p) {
+            const int d = rem % pl.r[p];
+            rem /= pl.r[p];
+            block /= pl.r[p];
+            pos += d * block;
+        }
+        f[pos] = k;
+    }
+    return f;
+}
+
+// dst[natural] = src[position] (to_natural) or dst[position] = src[natural].
+template <typename T, int MS>
+__global__ void k_permute(StepConst c, const cx<T>* src, cx<T>* dst, int to_natural) {
+    const long long np = c.npts;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < np; t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t % c.nx);
+        const long long rr = t / c.nx;
+        const int j = (int)(rr % c.ny), k = (int)(rr / c.ny);
+        const long long nat = c.fx[i] + (long long)c.nx * (c.fy[j] + (long long)c.ny * c.fz[k]);
+#pragma unroll
+        for (int m = 0; m < MS; ++m) {
+            if (to_natural) dst[(size_t)m * np + nat] = src[(size_t)m * np + t];
+            else dst[(size_t)m * np + t] = src[(size_t)m * np + nat];
+        }
+    }
+}
+
+template <typename T, int MS>
+void launch_permute(fgpe_t* h, int to_natural) {
+    k_permute<T, MS><<<148 * 8, 256, 0, h->st>>>(h->sc, (const cx<T>*)h->psi, (cx<T>*)h->S, to_natural);
+    h->launches++;
+    std::swap(h->psi, h->S);
+}
+
+int materialize(fgpe_t* h) {
+    if (h->psi_valid) return FGPE_OK;
+    if (!h->S_valid) return fail(h, FGPE_E_STATE, "no state set");
+    DISPATCH(h, launch_row, h, ROW_INV, nullptr);
+    CK(cudaGetLastError());
+    h->psi_valid = true;
+    return FGPE_OK;
+}
+
+int sync_info_err(fgpe_t* h, const double* dinfo) {
+    CK(cudaMemcpyAsync(h->h_small, dinfo, sizeof(double) * INFO_LEN, cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    return FGPE_OK;
+}
+
+}  // namespace
+
+// =================================================================== API
+extern "C" {
+
+int fgpe_version(void) { return 10000; }
+
+int fgpe_device_ok(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return 0;
+    int dev = 0; cudaGetDevice(&dev);
+    cudaDeviceProp pr;
+    if (cudaGetDeviceProperties(&pr, dev) != cudaSuccess) return 0;
+    return pr.major == 10 ? 1 : 0;
+}
+
+const char* fgpe_last_error(const fgpe_t* h) { return h ? h->msg.c_str() : g_last_error.c_str(); }
+
+int fgpe_create(const fgpe_params* pin, fgpe_t** out) {
+    fgpe_t* h = nullptr;
+    if (!pin || !out) return fail(h, FGPE_E_ARG, "null argument");
+    fgpe_params p = *pin;
+    if (p.dim < 1 || p.dim > 3) return fail(h, FGPE_E_ARG, "dim must be 1, 2 or 3");
+    if (p.spin != 1 && p.spin != 2) return fail(h, FGPE_E_ARG, "spin must be 1 or 2");
+    if (p.dim < 2) { p.ny = 1; p.dy = 1.0; }
+    if (p.dim < 3) { p.nz = 1; p.dz = 1.0; }
+    const int ns[3] = {p.nx, p.ny, p.nz};
+    for (int a = 0; a < p.dim; ++a)
+        if (ns[a] < 8 || ns[a] % 2) return fail(h, FGPE_E_ARG, "grid sizes must be even and >= 8 (Simpson rule)");
+    if (!(p.dt > 0)) return fail(h, FGPE_E_ARG, "dt must be positive");
+    if (p.precision != FGPE_FP64 && p.precision != FGPE_FP32) return fail(h, FGPE_E_ARG, "unknown precision");
+    if (!fgpe_device_ok()) return fail(h, FGPE_E_CUDA, "no sm_100 CUDA device available");
+
+    h = new fgpe_s();
+    h->p = p;
+    h->ms = 2 * p.spin + 1;
+    h->npts = (long long)p.nx * p.ny * p.nz;
+    h->fp32 = p.precision == FGPE_FP32;
+    h->cs = h->fp32 ? 8 : 16;
+    StepConst& c = h->sc;
+    memset(&c, 0, sizeof(c));
+    c.dim = p.dim; c.spin = p.spin; c.ms = h->ms;
+    c.nx = p.nx; c.ny = p.ny; c.nz = p.nz; c.npts = h->npts;
+    c.dt = p.dt; c.imag = p.imag_time ? 1 : 0;
+    c.tau0 = p.tau[0]; c.tau1 = p.tau[1]; c.tau2 = p.tau[2];
+    c.gx = p.gamma[0]; c.gy = p.dim >= 2 ? p.gamma[1] : 0.0; c.gz = p.dim >= 3 ? p.gamma[2] : 0.0;
+    c.se_half = (p.dim == 1 && p.spin == 2);
+    c.se_ge = (p.dim == 1);
+    for (int a = 0; a < 3; ++a) {
+        FftPlan* pl = a == 0 ? &c.px : a == 1 ? &c.py : &c.pz;
+        if (!plan_fft(ns[a], pl)) {
+            delete h;
+            return fail(nullptr, FGPE_E_ARG, "grid size " + std::to_string(ns[a]) + " is not of the form 2^a 3^b 5^c");
+        }
+    }
+
+    // ---- host tables
+    const double L[3] = {p.nx * p.dx, p.ny * p.dy, p.nz * p.dz};
+    const double dd[3] = {p.dx, p.dy, p.dz};
+    const double al[3] = {p.alpha[0], p.alpha[1], p.alpha[2]};
+    std::vector<double> dt_all;
+    size_t off_k[3], off_x[3], off_w[3], off_v[3];
+    for (int a = 0; a < 3; ++a) {
+        const int n = ns[a];
+        std::vector<double> k(n), x(n), w, v(n);
+        // cgpe1d.f90:692-704
+        if (a < p.dim) {
+            for (int i = 1; i <= 1 + n / 2; ++i) k[i - 1] = (i - 1.0) * 2.0 * kPi / L[a];
+            for (int i = 1; i <= n / 2 - 1; ++i) k[i + n / 2] = -k[n / 2 - i];
+            for (int i = 1; i <= n; ++i) x[i - 1] = (-1.0 + 2.0 * (i - 1.0) / n) * L[a] / 2.0;
+            w = simpson_weights(n, dd[a]);
+            for (int i = 0; i < n; ++i) v[i] = al[a] * al[a] * (x[i] * x[i]);
+        } else {
+            k[0] = 0; x[0] = 0; w.assign(1, 1.0); v[0] = 0;
+        }
+        off_k[a] = dt_all.size(); dt_all.insert(dt_all.end(), k.begin(), k.end());
+        off_x[a] = dt_all.size(); dt_all.insert(dt_all.end(), x.begin(), x.end());
+        off_w[a] = dt_all.size(); dt_all.insert(dt_all.end(), w.begin(), w.end());
+        off_v[a] = dt_all.size(); dt_all.insert(dt_all.end(), v.begin(), v.end());
+    }
+    // complex tables (as doubles; converted to T below)
+    std::vector<double> ct;
+    size_t off_tw[3], off_ke[3];
+    auto phase = [&](double xx, double* re, double* im) {  // exp(-i CDT xx)
+        if (p.imag_time) { *re = exp(-p.dt * xx); *im = 0.0; }
+        else { *re = cos(p.dt * xx); *im = -sin(p.dt * xx); }
+    };
+    for (int a = 0; a < 3; ++a) {
+        const int n = ns[a];
+        off_tw[a] = ct.size() / 2;
+        for (int t = 0; t < n; ++t) {
+            const double ang = -2.0 * kPi * (double)t / (double)n;
+            ct.push_back(cos(ang)); ct.push_back(sin(ang));
+        }
+    }
+    for (int a = 0; a < 3; ++a) {
+        const int n = ns[a];
+        const double* k = &dt_all[off_k[a]];
+        off_ke[a] = ct.size() / 2;
+        if (a < 2 || p.dim < 3) {
+            for (int i = 0; i < n; ++i) {
+                double re, im;
+                phase(a < p.dim ? k[i] * k[i] : 0.0, &re, &im);
+                ct.push_back(re); ct.push_back(im);
+            }
+        } else {
+            // 3D: exp(-i CDT (kz^2 - 2 L gz kz)), L = m - SPIN (cgpe3d.f90:892)
+            for (int m = 0; m < h->ms; ++m) {
+                const int Lm = m - p.spin;
+                for (int i = 0; i < n; ++i) {
+                    double re, im;
+                    phase(k[i] * k[i] - 2.0 * Lm * p.gamma[2] * k[i], &re, &im);
+                    ct.push_back(re); ct.push_back(im);
+                }
+            }
+        }
+    }
+
+    CK(cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking));
+    h->own_stream = true;
+    {
+        std::vector<int> pm;
+        size_t offp[3];
+        for (int a = 0; a < 3; ++a) {
+            const FftPlan& pl = a == 0 ? c.px : a == 1 ? c.py : c.pz;
+            std::vector<int> f = position_map(pl);
+            offp[a] = pm.size();
+            pm.insert(pm.end(), f.begin(), f.end());
+        }
+        CK(cudaMalloc(&h->pmap, pm.size() * sizeof(int)));
+        CK(cudaMemcpy(h->pmap, pm.data(), pm.size() * sizeof(int), cudaMemcpyHostToDevice));
+        c.fx = h->pmap + offp[0]; c.fy = h->pmap + offp[1]; c.fz = h->pmap + offp[2];
+    }
+    const size_t bytes = (size_t)h->npts * h->ms * h->cs;
+    CK(cudaMalloc(&h->S, bytes));
+    CK(cudaMalloc(&h->psi, bytes));
+    CK(cudaMalloc(&h->prev, bytes));
+    CK(cudaMalloc(&h->dtab, dt_all.size() * sizeof(double)));
+    CK(cudaMemcpy(h->dtab, dt_all.data(), dt_all.size() * sizeof(double), cudaMemcpyHostToDevice));
+    if (h->fp32) {
+        std::vector<float> f(ct.begin(), ct.end());
+        CK(cudaMalloc(&h->ctab, f.size() * sizeof(float)));
+        CK(cudaMemcpy(h->ctab, f.data(), f.size() * sizeof(float), cudaMemcpyHostToDevice));
+    } else {
+        CK(cudaMalloc(&h->ctab, ct.size() * sizeof(double)));
+        CK(cudaMemcpy(h->ctab, ct.data(), ct.size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    const size_t ces = h->cs;  // bytes per complex table entry
+    c.kx = h->dtab + off_k[0]; c.ky = h->dtab + off_k[1]; c.kz = h->dtab + off_k[2];
+    c.xg = h->dtab + off_x[0]; c.yg = h->dtab + off_x[1]; c.zg = h->dtab + off_x[2];
+    c.wx = h->dtab + off_w[0]; c.wy = h->dtab + off_w[1]; c.wz = h->dtab + off_w[2];
+    c.vx = h->dtab + off_v[0]; c.vy = h->dtab + off_v[1]; c.vz = h->dtab + off_v[2];
+    c.twx = (char*)h->ctab + off_tw[0] * ces; c.twy = (char*)h->ctab + off_tw[1] * ces; c.twz = (char*)h->ctab + off_tw[2] * ces;
+    c.kex = (char*)h->ctab + off_ke[0] * ces; c.key = (char*)h->ctab + off_ke[1] * ces; c.kez = (char*)h->ctab + off_ke[2] * ces;
+
+    // ---- launch shapes
+    const size_t budget = 100 * 1024;   // two blocks per SM
+    const size_t hard = 200 * 1024;     // one block per SM
+    const int ms = h->ms;
+    if (p.dim == 1) {
+        const int lp = padded_len(p.nx);
+        h->k1.smem = (size_t)ms * lp * h->cs;
+        h->k1.T = 512;
+        if (h->k1.smem > hard) {
+            fgpe_destroy(h);
+            return fail(nullptr, FGPE_E_ARG, "1D grid too large for the single-block kernel (NX*M*bytes must fit 200 KB)");
+        }
+    }
+    {
+        // row pass: R rows per block, R | NY*NZ
+        const int rows = p.ny * p.nz;
+        const int lp = padded_len(p.nx);
+        int best = 0;
+        for (int R = 1; R <= rows && R <= 64; ++R) {
+            if (rows % R) continue;
+            const size_t sm = (size_t)ms * R * lp * h->cs;
+            if (sm > (R == 1 ? hard : budget)) break;
+            best = R;
+            if ((size_t)ms * R * p.nx >= 2048) break;   // enough work per block
+        }
+        if (!best) { fgpe_destroy(h); return fail(nullptr, FGPE_E_ARG, "x lines too long for the row kernel"); }
+        h->row.tile = best;
+        h->row.smem = (size_t)ms * best * lp * h->cs;
+        h->row.T = 256;
+        h->row.grid = dim3(rows / best);
+    }
+    for (int a = 1; a < p.dim; ++a) {
+        const int n = ns[a];
+        const int lpn = padded_len(n);
+        int best = 0;
+        for (int TX = 1; TX <= 16 && TX <= p.nx; TX *= 2) {
+            if (p.nx % TX) break;
+            const size_t sm = (size_t)ms * lpn * TX * h->cs;
+            if (sm > (TX == 1 ? hard : budget)) break;
+            best = TX;
+            if ((size_t)TX * h->cs >= 32) break;          // whole 32-byte sectors per line
+        }
+        if (!best) { fgpe_destroy(h); return fail(nullptr, FGPE_E_ARG, "lines too long for the column kernel"); }
+        h->col[a].tile = best;
+        h->col[a].smem = (size_t)ms * lpn * best * h->cs;
+        h->col[a].T = 256;
+        const int other = p.dim == 2 ? 1 : (a == 1 ? p.nz : p.ny);
+        h->col[a].grid = dim3(p.nx / best, other);
+    }
+    h->obsl.grid = dim3((unsigned)((h->npts + 255) / 256));
+    const size_t nq = 3 * ms + 3;
+    const size_t npart = std::max<size_t>((size_t)h->obsl.grid.x * nq, (size_t)h->row.grid.x * ms) + 64;
+    CK(cudaMalloc(&h->part, npart * sizeof(double)));
+    CK(cudaMalloc(&h->info, 4 * INFO_LEN * sizeof(double)));
+    h->info_prev = h->info + INFO_LEN;
+    h->obs = h->info + 2 * INFO_LEN;
+    CK(cudaMalloc(&h->counters, 4 * sizeof(unsigned)));
+    CK(cudaMemset(h->counters, 0, 4 * sizeof(unsigned)));
+    CK(cudaMallocHost(&h->h_small, 64 * sizeof(double)));
+    std::vector<double> info0(4 * INFO_LEN, 0.0);
+    info0[INFO_SCALE] = 1.0; info0[INFO_LEN + INFO_SCALE] = 1.0;
+    CK(cudaMemcpy(h->info, info0.data(), info0.size() * sizeof(double), cudaMemcpyHostToDevice));
+    if (h->fp32) { set_smem_attrs<float, 3>(); set_smem_attrs<float, 5>(); }
+    else { set_smem_attrs<double, 3>(); set_smem_attrs<double, 5>(); }
+    CK(cudaGetLastError());
+    *out = h;
+    return FGPE_OK;
+}
+
+int fgpe_destroy(fgpe_t* h) {
+    if (!h) return FGPE_OK;
+    if (h->st) cudaStreamSynchronize(h->st);
+    cudaFree(h->S); cudaFree(h->psi); cudaFree(h->prev); cudaFree(h->stage);
+    cudaFree(h->dtab); cudaFree(h->ctab); cudaFree(h->part); cudaFree(h->info);
+    cudaFree(h->counters); cudaFree(h->pmap);
+    if (h->h_small) cudaFreeHost(h->h_small);
+    for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
+    if (h->own_stream && h->st) cudaStreamDestroy(h->st);
+    delete h;
+    return FGPE_OK;
+}
+
+int fgpe_set_stream(fgpe_t* h, void* stream) {
+    if (!h) return fail(h, FGPE_E_ARG, "null handle");
+    CK(cudaStreamSynchronize(h->st));
+    if (h->own_stream) cudaStreamDestroy(h->st);
+    if (stream) { h->st = (cudaStream_t)stream; h->own_stream = false; }
+    else { CK(cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking)); h->own_stream = true; }
+    return FGPE_OK;
+}
+
+static int ensure_stage(fgpe_t* h) {
+    if (h->stage) return FGPE_OK;
+    CK(cudaMalloc(&h->stage, (size_t)h->npts * h->ms * 16));
+    return FGPE_OK;
+}
+
+static int import_dev(fgpe_t* h, const void* src_dev) {
+    const long long n2 = h->npts * h->ms * 2;
+    if (h->fp32) {
+        k_import<float><<<148 * 8, 256, 0, h->st>>>((const double*)src_dev, (float*)h->psi, n2);
+        h->launches++;
+    } else {
+        CK(cudaMemcpyAsync(h->psi, src_dev, (size_t)n2 * 8, cudaMemcpyDeviceToDevice, h->st));
+    }
+    double one[INFO_LEN] = {0};
+    one[INFO_SCALE] = 1.0;   // pageable source: staged before the call returns
+    CK(cudaMemcpyAsync(h->info, one, sizeof(one), cudaMemcpyHostToDevice, h->st));
+    CK(cudaMemcpyAsync(h->info_prev, one, sizeof(one), cudaMemcpyHostToDevice, h->st));
+    CK(cudaGetLastError());
+    h->psi_valid = true; h->S_valid = false; h->prev_valid = false; h->norms_valid = false; h->has_state = true;
+    return FGPE_OK;
+}
+
+int fgpe_set_state(fgpe_t* h, const double* phi) {
+    if (!h || !phi) return fail(h, FGPE_E_ARG, "null argument");
+    const size_t bytes = (size_t)h->npts * h->ms * 16;
+    if (h->fp32) {
+        int r = ensure_stage(h); if (r) return r;
+        CK(cudaMemcpyAsync(h->stage, phi, bytes, cudaMemcpyHostToDevice, h->st));
+        return import_dev(h, h->stage);
+    }
+    CK(cudaMemcpyAsync(h->psi, phi, bytes, cudaMemcpyHostToDevice, h->st));
+    double one[INFO_LEN] = {0};
+    one[INFO_SCALE] = 1.0;
+    CK(cudaMemcpyAsync(h->info, one, sizeof(one), cudaMemcpyHostToDevice, h->st));
+    CK(cudaMemcpyAsync(h->info_prev, one, sizeof(one), cudaMemcpyHostToDevice, h->st));
+    h->psi_valid = true; h->S_valid = false; h->prev_valid = false; h->norms_valid = false; h->has_state = true;
+    return FGPE_OK;
+}
+
+int fgpe_set_state_device(fgpe_t* h, const void* phi_dev) {
+    if (!h || !phi_dev) return fail(h, FGPE_E_ARG, "null argument");
+    return import_dev(h, phi_dev);
+}
+
+static int export_to(fgpe_t* h, void* dst, cudaMemcpyKind kind) {
+    if (!h->has_state) return fail(h, FGPE_E_STATE, "no state set");
+    int r = materialize(h); if (r) return r;
+    r = ensure_stage(h); if (r) return r;
+    const long long n2 = h->npts * h->ms * 2;
+    if (h->fp32) k_export<float><<<148 * 8, 256, 0, h->st>>>((const float*)h->psi, (double*)h->stage, n2, h->info);
+    else k_export<double><<<148 * 8, 256, 0, h->st>>>((const double*)h->psi, (double*)h->stage, n2, h->info);
+    h->launches++;
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(dst, h->stage, (size_t)n2 * 8, kind, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    return check_err(h);
+}
+
+int fgpe_get_state(fgpe_t* h, double* phi) {
+    if (!h || !phi) return fail(h, FGPE_E_ARG, "null argument");
+    return export_to(h, phi, cudaMemcpyDeviceToHost);
+}
+
+int fgpe_get_state_device(fgpe_t* h, void* phi_dev) {
+    if (!h || !phi_dev) return fail(h, FGPE_E_ARG, "null argument");
+    return export_to(h, phi_dev, cudaMemcpyDeviceToDevice);
+}
+
+int fgpe_step_ex(fgpe_t* h, int nsteps, int flags) {
+    if (!h) return fail(h, FGPE_E_ARG, "null handle");
+    if (!h->has_state) return fail(h, FGPE_E_STATE, "no state set");
+    if (nsteps <= 0) return FGPE_OK;
+    const bool snap = !(flags & FGPE_STEP_NO_SNAPSHOT);
+    if (h->p.dim == 1) {
+        // the state of a 1D handle always lives in psi
+        int done = 0;
+        while (done < nsteps) {
+            const int chunk = std::min(4096, nsteps - done);
+            const bool last = done + chunk == nsteps;
+            void* sp = nullptr;
+            if (last) {
+                if (chunk == 1) {
+                    CK(cudaMemcpyAsync(h->prev, h->psi, (size_t)h->npts * h->ms * h->cs, cudaMemcpyDeviceToDevice, h->st));
+                    CK(cudaMemcpyAsync(h->info_prev, h->info, INFO_LEN * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
+                } else {
+                    sp = h->prev;
+                }
+            }
+            DISPATCH(h, launch_1d, h, chunk, sp);
+            CK(cudaGetLastError());
+            done += chunk;
+        }
+        h->prev_valid = true; h->psi_valid = true; h->norms_valid = true;
+        return FGPE_OK;
+    }
+    if (!h->S_valid) {
+        if (!h->psi_valid) return fail(h, FGPE_E_STATE, "no state set");
+        DISPATCH(h, launch_row, h, ROW_FWD, nullptr);
+        CK(cudaGetLastError());
+        h->S_valid = true;
+    }
+    h->prev_valid = false;
+    if (snap && h->psi_valid) {
+        std::swap(h->psi, h->prev);
+        CK(cudaMemcpyAsync(h->info_prev, h->info, INFO_LEN * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
+        h->prev_valid = true;
+    }
+    h->psi_valid = false;
+    for (int s = 0; s < nsteps; ++s) {
+        if (h->p.dim == 2) {
+            DISPATCH(h, launch_col, h, 1, COL_SCALE | COL_FWD | COL_KOP | COL_INV);
+        } else {
+            DISPATCH(h, launch_col, h, 1, COL_SCALE | COL_FWD);
+            DISPATCH(h, launch_col, h, 2, COL_FWD | COL_KOP | COL_INV);
+            DISPATCH(h, launch_col, h, 1, COL_INV);
+        }
+        void* sn = nullptr;
+        if (snap && s == nsteps - 1) sn = h->psi;
+        if (snap && s == nsteps - 2) sn = h->prev;
+        DISPATCH(h, launch_row, h, ROW_FULL, sn);
+        if (snap && s == nsteps - 2) {
+            CK(cudaMemcpyAsync(h->info_prev, h->info, INFO_LEN * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
+            h->prev_valid = true;
+        }
+    }
+    CK(cudaGetLastError());
+    h->psi_valid = snap;
+    h->norms_valid = true;
+    return FGPE_OK;
+}
+
+int fgpe_step(fgpe_t* h, int nsteps) { return fgpe_step_ex(h, nsteps, FGPE_STEP_DEFAULT); }
+
+int fgpe_normalize(fgpe_t* h, double* tnorm) {
+    if (!h) return fail(h, FGPE_E_ARG, "null handle");
+    if (!h->has_state) return fail(h, FGPE_E_STATE, "no state set");
+    int r = materialize(h); if (r) return r;
+    DISPATCH(h, launch_obs, h, OBS_NORMALIZE, false);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(h->h_small, h->obs, OBS_LEN * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    const double tot = h->h_small[OBS_TOTAL];
+    if (!(tot == tot) || !(tot > 0) || !(tot < 1e300)) return fail(h, FGPE_E_NONFINITE, "non-finite or zero total norm");
+    if (tnorm) *tnorm = sqrt(tot);
+    return check_err(h);
+}
+
+int fgpe_norms(fgpe_t* h, double* norm) {
+    if (!h || !norm) return fail(h, FGPE_E_ARG, "null argument");
+    if (!h->has_state) return fail(h, FGPE_E_STATE, "no state set");
+    if (h->norms_valid) {
+        int r = sync_info_err(h, h->info); if (r) return r;
+        for (int m = 0; m < h->ms; ++m) norm[m] = h->h_small[INFO_NORM + m];
+        if (h->h_small[INFO_ERR] != 0.0) return fail(h, FGPE_E_NONFINITE, "non-finite norm in a step");
+        return check_err(h);
+    }
+    int r = materialize(h); if (r) return r;
+    DISPATCH(h, launch_obs, h, OBS_NORMS, false);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(h->h_small, h->obs, OBS_LEN * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    for (int m = 0; m < h->ms; ++m) norm[m] = h->h_small[OBS_NORM + m];
+    return check_err(h);
+}
+
+int fgpe_observables(fgpe_t* h, double* en, double* mu, double* mz, double* rms) {
+    if (!h) return fail(h, FGPE_E_ARG, "null handle");
+    if (!h->has_state) return fail(h, FGPE_E_STATE, "no state set");
+    int r = materialize(h); if (r) return r;
+    DISPATCH(h, launch_obs, h, OBS_FULL, false);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(h->h_small, h->obs, OBS_LEN * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    const double* o = h->h_small;
+    if (en) *en = o[OBS_EN];
+    if (mz) *mz = o[OBS_MZ];
+    for (int m = 0; m < h->ms; ++m) {
+        if (mu) mu[m] = o[OBS_MU + m];
+        if (rms) rms[m] = o[OBS_RMS + m];
+    }
+    if (!(o[OBS_EN] == o[OBS_EN])) return fail(h, FGPE_E_NONFINITE, "non-finite energy");
+    return check_err(h);
+}
+
+int fgpe_conv(fgpe_t* h, double* max_dphi) {
+    if (!h || !max_dphi) return fail(h, FGPE_E_ARG, "null argument");
+    if (!h->prev_valid) return fail(h, FGPE_E_STATE, "no previous-step snapshot (step with snapshots first)");
+    int r = materialize(h); if (r) return r;
+    DISPATCH(h, launch_obs, h, OBS_NORMS, true);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(h->h_small, h->obs, OBS_LEN * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    *max_dphi = h->h_small[OBS_CONV];
+    return check_err(h);
+}
+
+int fgpe_center(fgpe_t* h, double* out) {
+    if (!h || !out) return fail(h, FGPE_E_ARG, "null argument");
+    if (!h->has_state) return fail(h, FGPE_E_STATE, "no state set");
+    int r = materialize(h); if (r) return r;
+    const long long idx = (long long)(h->p.nx / 2) + (long long)h->p.nx * ((h->p.ny > 1 ? h->p.ny / 2 : 0) + (long long)h->p.ny * (h->p.nz > 1 ? h->p.nz / 2 : 0));
+    for (int m = 0; m < h->ms; ++m)
+        CK(cudaMemcpyAsync((char*)h->h_small + m * 16, (char*)h->psi + ((size_t)m * h->npts + idx) * h->cs, h->cs, cudaMemcpyDeviceToHost, h->st));
+    CK(cudaMemcpyAsync(h->h_small + 32, h->info, INFO_LEN * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    const double s = h->h_small[32 + INFO_SCALE];
+    for (int m = 0; m < h->ms; ++m) {
+        double re, im;
+        if (h->fp32) { float f[2]; memcpy(f, (char*)h->h_small + m * 16, 8); re = f[0]; im = f[1]; }
+        else { memcpy(&re, (char*)h->h_small + m * 16, 8); memcpy(&im, (char*)h->h_small + m * 16 + 8, 8); }
+        out[2 * m] = s * re; out[2 * m + 1] = s * im;
+    }
+    return FGPE_OK;
+}
+
+int fgpe_apply_op(fgpe_t* h, int op) {
+    if (!h) return fail(h, FGPE_E_ARG, "null handle");
+    if (!h->has_state) return fail(h, FGPE_E_STATE, "no state set");
+    int r = materialize(h); if (r) return r;
+    // fold the pending scale into psi
+    if (h->fp32) k_apply_scale<float><<<148 * 8, 256, 0, h->st>>>((float*)h->psi, h->npts * h->ms * 2, h->info);
+    else k_apply_scale<double><<<148 * 8, 256, 0, h->st>>>((double*)h->psi, h->npts * h->ms * 2, h->info);
+    h->launches++;
+    const double one = 1.0;   // pageable source: staged before the call returns
+    CK(cudaMemcpyAsync(h->info + INFO_SCALE, &one, sizeof(double), cudaMemcpyHostToDevice, h->st));
+    switch (op) {
+        case FGPE_OP_FFT: {
+            void* keep = h->S;
+            h->S = h->psi;                                    // in place
+            DISPATCH(h, launch_row, h, ROW_FWD, nullptr);
+            if (h->p.dim >= 2) DISPATCH(h, launch_col, h, 1, COL_FWD);
+            if (h->p.dim >= 3) DISPATCH(h, launch_col, h, 2, COL_FWD);
+            h->S = keep;
+            DISPATCH(h, launch_permute, h, 1);                // digit-reversed -> natural
+        } break;
+        case FGPE_OP_BFT: {
+            DISPATCH(h, launch_permute, h, 0);                // natural -> digit-reversed
+            void* keep = h->S;
+            h->S = h->psi;
+            if (h->p.dim >= 3) DISPATCH(h, launch_col, h, 2, COL_INV);
+            if (h->p.dim >= 2) DISPATCH(h, launch_col, h, 1, COL_INV);
+            DISPATCH(h, launch_row, h, ROW_INV, nullptr);     // psi <- F_x^-1[psi]/NX
+            h->S = keep;
+            if (h->p.dim >= 2) DISPATCH(h, launch_point, h, OP_SCALE, 1.0 / ((double)h->p.ny * h->p.nz));
+        } break;
+        case FGPE_OP_KE: DISPATCH(h, launch_point, h, OP_KE, 0.0); break;
+        case FGPE_OP_SOC: DISPATCH(h, launch_point, h, OP_SOC, 0.0); break;
+        case FGPE_OP_SE: DISPATCH(h, launch_point, h, OP_SE, 0.0); break;
+        case FGPE_OP_SP: DISPATCH(h, launch_point, h, OP_SP, 0.0); break;
+        default: return fail(h, FGPE_E_ARG, "unknown operator");
+    }
+    CK(cudaGetLastError());
+    h->psi_valid = true; h->S_valid = false; h->prev_valid = false; h->norms_valid = false;
+    return FGPE_OK;
+}
+
+int fgpe_norms_async(fgpe_t* h, double* dst) {
+    if (!h || !dst) return fail(h, FGPE_E_ARG, "null argument");
+    if (!h->norms_valid) return fail(h, FGPE_E_STATE, "no step taken since the state was set");
+    CK(cudaMemcpyAsync(dst, h->info + INFO_NORM, h->ms * sizeof(double), cudaMemcpyDefault, h->st));
+    return FGPE_OK;
+}
+
+int fgpe_profile_enable(fgpe_t* h, int on) {
+    if (!h) return fail(h, FGPE_E_ARG, "null handle");
+    h->prof = on != 0;
+    return FGPE_OK;
+}
+
+int fgpe_profile_read(fgpe_t* h, double* ms, long long* n, int reset) {
+    if (!h) return fail(h, FGPE_E_ARG, "null handle");
+    CK(cudaStreamSynchronize(h->st));
+    for (auto& r : h->ev_rec) {
+        float t = 0.f;
+        CK(cudaEventElapsedTime(&t, h->ev_pool[r.second], h->ev_pool[r.second + 1]));
+        h->prof_ms[r.first] += t;
+        h->prof_n[r.first] += 1;
+    }
+    h->ev_rec.clear();
+    for (int i = 0; i < 4; ++i) {
+        if (ms) ms[i] = h->prof_ms[i];
+        if (n) n[i] = h->prof_n[i];
+        if (reset) { h->prof_ms[i] = 0; h->prof_n[i] = 0; }
+    }
+    return FGPE_OK;
+}
+
+int fgpe_kernel_launches(fgpe_t* h, long long* count) {
+    if (!h || !count) return fail(h, FGPE_E_ARG, "null argument");
+    *count = h->launches;
+    return FGPE_OK;
+}
+
+}  // extern "C"

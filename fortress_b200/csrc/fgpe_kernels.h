@@ -1,0 +1,74 @@
+// fgpe_kernels.h -- argument blocks shared by the kernels and the host API.
+#pragma once
+#include "fgpe_device.cuh"
+
+namespace fgpe {
+
+// Layout of the per-handle device "info" vector (doubles).
+enum {
+    INFO_SCALE = 0,   // pending renormalisation: phi = scale * psi
+    INFO_TOTAL = 1,   // sum of the norms of the last step (before NORMT)
+    INFO_ERR = 2,     // non-finite reduction seen
+    INFO_NORM = 3,    // NORMC of the last step, MS values
+    INFO_LEN = 16
+};
+
+// Layout of the observables result vector.
+enum {
+    OBS_EN = 0, OBS_MZ = 1, OBS_CONV = 2, OBS_TOTAL = 3,
+    OBS_NORM = 4, OBS_MU = 9, OBS_RMS = 14, OBS_LEN = 20
+};
+
+enum { ROW_FULL = 0, ROW_FWD = 1, ROW_INV = 2 };
+enum { COL_SCALE = 1, COL_FWD = 2, COL_KOP = 4, COL_INV = 8 };
+enum { OBS_FULL = 0, OBS_NORMS = 1, OBS_NORMALIZE = 2 };
+enum { OP_KE = 1, OP_SOC = 2, OP_SE = 3, OP_SP = 4, OP_SCALE = 5 };
+
+struct RowArgs {
+    void* S;           // x-spectral spinor (in/out)
+    void* psi;         // real-space spinor (ROW_FWD source / ROW_INV target)
+    void* snap;        // ROW_FULL: optional real-space snapshot target
+    double* part;      // per-block NORMC partials
+    unsigned* counter; // last-block counter (zero between launches)
+    double* info;      // INFO_* vector
+    int rows;          // rows (x lines) per block
+    int mode;
+};
+
+struct ColArgs {
+    void* S;
+    const void* tw;    // twiddles of the transformed axis
+    FftPlan plan;
+    double* info;
+    double cfac;       // 1/(NX*NY*NZ) folded into the scale on load
+    long long axis_stride, other_stride;
+    int n, tx, flags;
+};
+
+struct OneDArgs {
+    void* psi;
+    void* snap_prev;
+    double* info;
+    double* info_prev;
+    int nsteps;
+};
+
+struct ObsArgs {
+    const void* psi;
+    const void* prev;
+    double* info;
+    const double* info_prev;
+    double* part;
+    unsigned* counter;
+    double* out;
+    double dx, dy, dz;
+    int mode;
+};
+
+struct PointArgs {
+    void* psi;
+    int op;
+    double factor;
+};
+
+}  // namespace fgpe

@@ -1,0 +1,145 @@
+/*
+ * fgpe.h -- C ABI of the B200 split-step spinor GPE propagator.
+ *
+ * The reference FORTRESS programs (SRC/cgpe1d.f90, cgpe2d.f90, cgpe3d.f90) keep
+ * the state in module globals PHI/PHIF and advance it with argument-less
+ * subroutines called from the main loop:
+ *     FFT, KE, SOC, BFT, SE, SP, NORMC, NORMT      (cgpe1d.f90:433-474)
+ *     ENERGY, RAD, CONV/CONV_EN                     (cgpe1d.f90:476-487)
+ * with their interfaces declared at cgpe1d.f90:117-198 (2D: cgpe2d.f90:118-200,
+ * 3D: cgpe3d.f90:122-205).  This header is the seam that replaces them: a
+ * handle owns the device-resident state, one call advances whole split steps
+ * (imaginary-time renormalisation included), and the observables come back as
+ * plain doubles.  A Fortran host binds it with ISO_C_BINDING.
+ *
+ * Conventions
+ *   - Every function returns 0 (FGPE_OK) on success and a negative FGPE_E*
+ *     code on failure; fgpe_last_error() gives a message for the handle.
+ *   - State arrays on the host are Fortran column-major PHI(NX,NY,NZ,M),
+ *     M = 2*SPIN+1, complex128 stored as interleaved (re, im) doubles, exactly
+ *     the reference's PHI layout.
+ *   - One host thread per handle; calls on a handle are ordered on the
+ *     handle's CUDA stream.  The library owns all device memory of a handle.
+ *   - There is no CPU fallback: without a usable sm_100 device every call that
+ *     needs the GPU fails with FGPE_E_CUDA.
+ */
+#ifndef FGPE_H
+#define FGPE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    FGPE_OK = 0,
+    FGPE_E_ARG = -1,        /* invalid argument / unsupported size */
+    FGPE_E_CUDA = -2,       /* CUDA runtime error (message in fgpe_last_error) */
+    FGPE_E_STATE = -3,      /* call out of order (e.g. no state set) */
+    FGPE_E_NONFINITE = -4   /* a reduction produced NaN/Inf */
+};
+
+enum { FGPE_FP64 = 0, FGPE_FP32 = 1 };
+
+/* Step flags for fgpe_step_ex. */
+enum {
+    FGPE_STEP_DEFAULT = 0,
+    FGPE_STEP_NO_SNAPSHOT = 1   /* keep the state in the spectral work buffer
+                                   only; the real-space copy is rebuilt lazily */
+};
+
+/* Physical and numerical parameters of one instance.  Field meanings follow
+ * the reference's input records (README.md:53-86) and derived quantities
+ * (cgpe1d.f90:263-271, 321-332). */
+typedef struct fgpe_params {
+    int dim;            /* 1, 2 or 3 (which cgpe{1,2,3}d program) */
+    int spin;           /* SPIN: 1 or 2 */
+    int nx, ny, nz;     /* NX, NY, NZ (unused dimensions = 1) */
+    double dx, dy, dz;  /* DX, DY, DZ */
+    double dt;          /* DT */
+    int imag_time;      /* SWITCH_IM: 1 imaginary time (CDT=-i DT), 0 real */
+    double tau[3];      /* TAU(0:2) in the reference's units (tau includes x2) */
+    double gamma[3];    /* GAMMAX, GAMMAY, GAMMAZ */
+    double alpha[3];    /* ALPHAX, ALPHAY, ALPHAZ = NU{X,Y,Z}/NUX */
+    int precision;      /* FGPE_FP64 or FGPE_FP32 (FP32 FFTs/exponentials,
+                           FP64 reductions and renormalisation) */
+    int reserved[7];
+} fgpe_params;
+
+typedef struct fgpe_s fgpe_t;
+
+/* Handle lifecycle.  Replaces ALLOCATE_MEM/INITIALIZE's grid set-up and
+ * CREATE_PLANS (cgpe1d.f90:568-589, 692-710, 796-807). */
+int fgpe_create(const fgpe_params *p, fgpe_t **out);
+int fgpe_destroy(fgpe_t *h);                      /* DEALLOCATE_MEM, DESTROY_PLANS */
+const char *fgpe_last_error(const fgpe_t *h);     /* NULL handle: last global error */
+int fgpe_set_stream(fgpe_t *h, void *cuda_stream);/* cudaStream_t, NULL = library's own */
+
+/* State transfer (host buffers, layout above).  Replaces the direct access to
+ * module PHI and the initial_sol reader's assignment (cgpe1d.f90:377-391). */
+int fgpe_set_state(fgpe_t *h, const double *phi_host);
+int fgpe_get_state(fgpe_t *h, double *phi_host);
+/* Device-pointer variants (complex128 or complex64 per precision is NOT used
+ * here: these always take complex128 in the same layout). */
+int fgpe_set_state_device(fgpe_t *h, const void *phi_dev);
+int fgpe_get_state_device(fgpe_t *h, void *phi_dev);
+
+/* Advance nsteps whole Lie split steps
+ *   FFT -> KE -> SOC -> BFT -> SE -> SP -> NORMC [-> NORMT if imaginary time]
+ * (cgpe1d.f90:433-474 for the SO-coupled branch). */
+int fgpe_step(fgpe_t *h, int nsteps);
+int fgpe_step_ex(fgpe_t *h, int nsteps, int flags);
+
+/* NORMT (cgpe1d.f90:998-1031): divide the state by sqrt(total Simpson norm);
+ * tnorm (may be NULL) receives TNORM. */
+int fgpe_normalize(fgpe_t *h, double *tnorm);
+
+/* NORMC of the state after the last step's SP, before renormalisation
+ * (cgpe1d.f90:441; what file1/file3 report).  Before any step: NORMC of the
+ * current state.  norm[M]. */
+int fgpe_norms(fgpe_t *h, double *norm);
+
+/* ENERGY + RAD of the current state (cgpe1d.f90:1077-1240, 1036-1072):
+ * en, mu[M], mz, rms[M] exactly as the reference defines them (not halved). */
+int fgpe_observables(fgpe_t *h, double *en, double *mu, double *mz, double *rms);
+
+/* max |PHI - PHI_OLD| over all points and components, PHI_OLD being the state
+ * one step before the current one (cgpe1d.f90:482, without the STP*2*DT
+ * divisor).  Valid after an fgpe_step call of at least one step. */
+int fgpe_conv(fgpe_t *h, double *max_dphi);
+
+/* Component values at the grid centre PHI(NX/2+1, NY/2+1, NZ/2+1, :) (the
+ * |phi| columns of file1, cgpe1d.f90:407).  out[2*M] interleaved. */
+int fgpe_center(fgpe_t *h, double *out);
+
+/* Unfused single operators in the reference's order, for operator-level
+ * parity checks.  They act on the handle's state: FGPE_OP_FFT moves it to
+ * Fourier space (unnormalised), KE/SOC act there, FGPE_OP_BFT moves it back
+ * (divided by NX*NY*NZ), SE/SP act in real space.  Replaces the individual
+ * subroutines FFT/KE/SOC/BFT/SE/SP (cgpe1d.f90:1324, 826, 1504, 1343, 1363,
+ * 847). */
+enum { FGPE_OP_FFT = 1, FGPE_OP_KE = 2, FGPE_OP_SOC = 3, FGPE_OP_BFT = 4,
+       FGPE_OP_SE = 5, FGPE_OP_SP = 6 };
+int fgpe_apply_op(fgpe_t *h, int op);
+
+/* Non-blocking variant of fgpe_norms: enqueues the copy of the last step's
+ * NORMC (M doubles) into dst, which must be pinned host memory (or device
+ * memory) and is valid after the handle's stream has been synchronised. */
+int fgpe_norms_async(fgpe_t *h, double *dst);
+
+/* Kernel timing with CUDA events recorded on the handle's stream around
+ * every kernel that fgpe_step launches.  fgpe_profile_read synchronises,
+ * adds the elapsed times per kernel class -- [0] row pass (x), [1] column
+ * pass y, [2] column pass z, [3] single-block 1D kernel -- into ms[4] and the
+ * launch counts into n[4], and clears the record when reset != 0. */
+int fgpe_profile_enable(fgpe_t *h, int on);
+int fgpe_profile_read(fgpe_t *h, double *ms, long long *n, int reset);
+
+/* Library / device information. */
+int fgpe_version(void);
+int fgpe_device_ok(void);                /* 1 if an sm_100 device is usable */
+int fgpe_kernel_launches(fgpe_t *h, long long *count);  /* kernels launched */
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FGPE_H */

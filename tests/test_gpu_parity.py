@@ -1,0 +1,87 @@
+"""GPU path (libfgpe.so through the C ABI) against the CPU oracle on the same
+seeded inputs.  FP64 tolerances: states 1e-11 relative to max|phi| per step
+batch, observables 1e-10 relative; FP32 bulk path: 2e-5."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests.helpers import CASES, case_id, case_params, initial_state, oracle_kwargs, rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def F():
+    import fortress_b200 as F
+    if not F.device_ok():
+        pytest.fail("no usable sm_100 device / libfgpe.so not loaded")
+    return F
+
+
+def _pair(F, case, precision="fp64", seed=0):
+    p = case_params(case)
+    orc = O.Oracle(**oracle_kwargs(p))
+    phi = initial_state(orc, seed)
+    orc.set_state(phi)
+    prop = F.Propagator(**p, precision=precision)
+    prop.set_state(phi)
+    return orc, prop
+
+
+@pytest.mark.parametrize("case", CASES, ids=case_id)
+@pytest.mark.parametrize("op", ["FFT", "KE", "SOC", "BFT", "SE", "SP"])
+def test_operator(F, case, op):
+    orc, prop = _pair(F, case)
+    if op in ("KE", "SOC", "BFT"):
+        orc.fft(); prop.FFT()
+    getattr(orc, op.lower())()
+    getattr(prop, op)()
+    assert rel_err(prop.state(), orc.state()) < 1e-12
+
+
+@pytest.mark.parametrize("case", CASES, ids=case_id)
+def test_steps(F, case):
+    orc, prop = _pair(F, case)
+    dim, spin, imag, n = case
+    if imag:
+        orc.normt(); prop.normt()
+    for batch in (1, 7):
+        prev = orc.state()
+        norm_o = orc.step(batch)
+        prop.step(batch)
+        assert rel_err(prop.state(), orc.state()) < 1e-11
+        assert np.allclose(prop.normc(), norm_o, rtol=1e-11, atol=0)
+        en_g, mu_g, mz_g, rms_g = prop.observables()
+        en_o, mu_o, mz_o = orc.energy()
+        assert abs(en_g - en_o) <= 1e-10 * abs(en_o)
+        assert np.allclose(mu_g, mu_o, rtol=1e-10, atol=1e-12)
+        assert abs(mz_g - mz_o) <= 1e-10 * max(1.0, abs(mz_o))
+        assert np.allclose(rms_g, orc.rad(), rtol=1e-10, atol=0)
+        if batch == 1:
+            c_o = orc.maxdiff(prev)
+            assert abs(prop.conv() - c_o) <= 1e-9 * c_o + 1e-15
+
+
+@pytest.mark.parametrize("case", [CASES[i] for i in (1, 5, 6, 9)], ids=case_id)
+def test_fp32_bulk(F, case):
+    orc, prop = _pair(F, case, precision="fp32")
+    dim, spin, imag, n = case
+    if imag:
+        orc.normt(); prop.normt()
+    orc.step(10)
+    prop.step(10)
+    assert rel_err(prop.state(), orc.state()) < 2e-5
+    en_g, mu_g, mz_g, rms_g = prop.observables()
+    en_o, mu_o, mz_o = orc.energy()
+    assert abs(en_g - en_o) <= 2e-5 * abs(en_o)
+    assert np.allclose(rms_g, orc.rad(), rtol=2e-5)
+
+
+def test_error_paths(F):
+    with pytest.raises(F.FgpeError):
+        F.Propagator(dim=2, spin=1, n=(32, 14), d=(0.1, 0.1), dt=1e-3, imag_time=1, tau=(1, 0, 0))  # 14 = 2*7 has a factor outside {2,3,5}
+    with pytest.raises(F.FgpeError):
+        F.Propagator(dim=2, spin=3, n=(32, 32), d=(0.1, 0.1), dt=1e-3, imag_time=1, tau=(1, 0, 0))
+    p = F.Propagator(dim=2, spin=1, n=(32, 32), d=(0.1, 0.1), dt=1e-3, imag_time=1, tau=(1, 0, 0))
+    with pytest.raises(F.FgpeError):
+        p.step(1)      # no state set
