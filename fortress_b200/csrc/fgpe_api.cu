@@ -123,10 +123,22 @@ std::vector<double> simpson_weights(int n, double dx) {
     return w;
 }
 
-template <typename T, int MS> void set_smem_attrs() {
-    cudaFuncSetAttribute(k_row<T, MS>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-    cudaFuncSetAttribute(k_col<T, MS>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-    cudaFuncSetAttribute(k_1d<T, MS>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+// Allow each kernel the opt-in shared-memory maximum minus its static part.
+template <class K> cudaError_t allow_smem(K kern) {
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, kern);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
+}
+
+template <typename T, int MS> cudaError_t set_smem_attrs() {
+    cudaError_t e = allow_smem(k_row<T, MS>);
+    if (e == cudaSuccess) e = allow_smem(k_col<T, MS>);
+    if (e == cudaSuccess) e = allow_smem(k_1d<T, MS>);
+    return e;
 }
 
 // Event pair around one launch when profiling is on.
@@ -507,8 +519,12 @@ int fgpe_create(const fgpe_params* pin, fgpe_t** out) {
     std::vector<double> info0(4 * INFO_LEN, 0.0);
     info0[INFO_SCALE] = 1.0; info0[INFO_LEN + INFO_SCALE] = 1.0;
     CK(cudaMemcpy(h->info, info0.data(), info0.size() * sizeof(double), cudaMemcpyHostToDevice));
-    if (h->fp32) { set_smem_attrs<float, 3>(); set_smem_attrs<float, 5>(); }
-    else { set_smem_attrs<double, 3>(); set_smem_attrs<double, 5>(); }
+    {
+        cudaError_t e1 = h->fp32 ? set_smem_attrs<float, 3>() : set_smem_attrs<double, 3>();
+        cudaError_t e2 = h->fp32 ? set_smem_attrs<float, 5>() : set_smem_attrs<double, 5>();
+        CK(e1);
+        CK(e2);
+    }
     CK(cudaGetLastError());
     *out = h;
     return FGPE_OK;
