@@ -187,6 +187,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--prep-steps", type=int, default=3000,
+                    help="imaginary-time relaxation steps that build the initial state (untimed)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -210,10 +212,12 @@ def main():
 
     cfg_gs = workload_config(WORKLOAD["gamma_gs"])
     cfg = workload_config(WORKLOAD["gamma"])
-    phi0 = prepared_state(F, cfg_gs)
+    phi0 = prepared_state(F, cfg_gs, args.prep_steps)
 
     prop = F.Propagator(**cfg.params(args.precision))
-    stream = torch.cuda.current_stream()
+    # a real (non-default) stream shared by torch's events and the library
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     prop.set_stream(stream.cuda_stream)
     prop.set_state(phi0)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")

@@ -10,7 +10,9 @@ import ctypes
 import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libfgpe.so")
+# FGPE_LIB_PATH selects an alternative build of the same library (for example
+# a diagnostic build); the default is the in-tree libfgpe.so.
+LIB_PATH = os.environ.get("FGPE_LIB_PATH") or os.path.join(_HERE, "libfgpe.so")
 
 FGPE_OK = 0
 FGPE_E_ARG = -1
@@ -48,7 +50,7 @@ class Params(ctypes.Structure):
                 ("dt", ctypes.c_double), ("imag_time", ctypes.c_int),
                 ("tau", ctypes.c_double * 3), ("gamma", ctypes.c_double * 3),
                 ("alpha", ctypes.c_double * 3), ("precision", ctypes.c_int),
-                ("reserved", ctypes.c_int * 7)]
+                ("kernels", ctypes.c_int), ("reserved", ctypes.c_int * 6)]
 
 
 _LIB = None

@@ -18,6 +18,7 @@
 
 #include "../../include/fgpe.h"
 #include "fgpe_kernels.cuh"
+#include "fgpe_fast.cuh"
 
 using namespace fgpe;
 
@@ -52,6 +53,8 @@ struct fgpe_s {
     void* ctab = nullptr;
     double* h_small = nullptr;   // pinned, 64 doubles
     Launch row, col[3], k1, obsl;
+    bool fast_row = false, fast_col[3] = {false, false, false};
+    int fast_row_grid = 0, fast_col_grid[3] = {0, 0, 0};
     bool psi_valid = false, S_valid = false, prev_valid = false, norms_valid = false, has_state = false;
     long long launches = 0;
     std::string msg;
@@ -134,11 +137,74 @@ template <class K> cudaError_t allow_smem(K kern) {
     return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
 }
 
+template <class K> cudaError_t allow_smem_exact(K kern, size_t bytes) {
+    return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
 template <typename T, int MS> cudaError_t set_smem_attrs() {
     cudaError_t e = allow_smem(k_row<T, MS>);
     if (e == cudaSuccess) e = allow_smem(k_col<T, MS>);
     if (e == cudaSuccess) e = allow_smem(k_1d<T, MS>);
     return e;
+}
+
+// ------------------------------------------------ specialised fast kernels
+// Line lengths with compiled persistent kernels; other sizes use the generic
+// kernels (same layout and results).
+constexpr int kFastN[] = {128, 192, 256, 384, 512};
+
+template <typename T> constexpr int col_tx() { return sizeof(T) == 8 ? 2 : 4; }
+constexpr int row_r(int n) { return n >= 384 ? 1 : 512 / n; }
+constexpr int fast_threads(int tot) {
+    const int iter = (tot + 511) / 512;
+    const int per = (tot + iter - 1) / iter;
+    return (per + 31) / 32 * 32;
+}
+template <typename T, int MS, int N> constexpr int row_th() { return fast_threads(MS * row_r(N) * N / 8); }
+template <typename T, int MS, int N> constexpr int col_th() { return fast_threads(MS * col_tx<T>() * N / 8); }
+template <typename T, int MS, int N> constexpr size_t row_smem() { return 2ull * MS * row_r(N) * cpad(N) * sizeof(cx<T>); }
+template <typename T, int MS, int N> constexpr size_t col_smem() { return 2ull * MS * cpad(N) * col_tx<T>() * sizeof(cx<T>); }
+
+template <class K> int grid_for(K kern, int th, size_t smem, int ntiles) {
+    int dev = 0, nsm = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (allow_smem_exact(kern, smem) != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, th, smem) != cudaSuccess || per < 1) return 0;
+    return std::min(ntiles, per * nsm);
+}
+
+template <typename T, int MS, int N> int setup_fast_row(fgpe_t* h) {
+    const int rows = h->p.ny * h->p.nz;
+    if (rows % row_r(N)) return 0;
+    return grid_for(k_row_fast<T, MS, N, row_r(N), row_th<T, MS, N>()>, row_th<T, MS, N>(), row_smem<T, MS, N>(),
+                    rows / row_r(N));
+}
+template <typename T, int MS, int N> int setup_fast_col(fgpe_t* h, int ntiles) {
+    if (h->p.nx % col_tx<T>()) return 0;
+    return grid_for(k_col_fast<T, MS, N, col_tx<T>(), col_th<T, MS, N>()>, col_th<T, MS, N>(), col_smem<T, MS, N>(),
+                    ntiles);
+}
+template <typename T, int MS, int N> void run_fast_row(fgpe_t* h, const RowArgs& a) {
+    k_row_fast<T, MS, N, row_r(N), row_th<T, MS, N>()><<<h->fast_row_grid, row_th<T, MS, N>(), row_smem<T, MS, N>(), h->st>>>(h->sc, a);
+}
+template <typename T, int MS, int N> void run_fast_col(fgpe_t* h, int axis, const ColArgs& a) {
+    k_col_fast<T, MS, N, col_tx<T>(), col_th<T, MS, N>()><<<h->fast_col_grid[axis], col_th<T, MS, N>(), col_smem<T, MS, N>(), h->st>>>(h->sc, a);
+}
+
+#define FAST_SWITCH(n, CALL)            \
+    switch (n) {                         \
+        case 128: CALL(128); break;      \
+        case 192: CALL(192); break;      \
+        case 256: CALL(256); break;      \
+        case 384: CALL(384); break;      \
+        case 512: CALL(512); break;      \
+        default: break;                  \
+    }
+
+bool fast_size(int n) {
+    for (int v : kFastN) if (v == n) return true;
+    return false;
 }
 
 // Event pair around one launch when profiling is on.
@@ -166,6 +232,13 @@ void launch_row(fgpe_t* h, int mode, void* snap) {
     a.S = h->S; a.psi = h->psi; a.snap = snap; a.part = h->part; a.counter = h->counters;
     a.info = h->info; a.rows = h->row.tile; a.mode = mode;
     ProfScope ps(h, 0);
+    if (h->fast_row) {
+#define RUNR(NN) run_fast_row<T, MS, NN>(h, a)
+        FAST_SWITCH(h->p.nx, RUNR)
+#undef RUNR
+        h->launches++;
+        return;
+    }
     k_row<T, MS><<<h->row.grid, h->row.T, h->row.smem, h->st>>>(h->sc, a);
     h->launches++;
 }
@@ -183,7 +256,15 @@ void launch_col(fgpe_t* h, int axis, int flags) {
     a.other_stride = h->p.dim == 2 ? 0 : (axis == 1 ? (long long)h->p.nx * h->p.ny : h->p.nx);
     a.tx = h->col[axis].tile;
     a.flags = flags;
+    a.n_other = h->p.dim == 2 ? 1 : (axis == 1 ? h->p.nz : h->p.ny);
     ProfScope ps(h, axis);
+    if (h->fast_col[axis]) {
+#define RUNC(NN) run_fast_col<T, MS, NN>(h, axis, a)
+        FAST_SWITCH(a.n, RUNC)
+#undef RUNC
+        h->launches++;
+        return;
+    }
     k_col<T, MS><<<h->col[axis].grid, h->col[axis].T, h->col[axis].smem, h->st>>>(h->sc, a);
     h->launches++;
 }
@@ -506,9 +587,32 @@ int fgpe_create(const fgpe_params* pin, fgpe_t** out) {
         const int other = p.dim == 2 ? 1 : (a == 1 ? p.nz : p.ny);
         h->col[a].grid = dim3(p.nx / best, other);
     }
+    // specialised persistent kernels where compiled for this size
+    const bool allow_fast = p.kernels != FGPE_KERNELS_GENERIC;
+    const bool allow_fast_row = allow_fast && p.kernels != FGPE_KERNELS_FAST_COL_ONLY;
+    const bool allow_fast_col = allow_fast && p.kernels != FGPE_KERNELS_FAST_ROW_ONLY;
+    if (allow_fast_row && p.dim >= 2 && fast_size(p.nx)) {
+        int g = 0;
+#define SETR(NN) g = h->fp32 ? (ms == 3 ? setup_fast_row<float, 3, NN>(h) : setup_fast_row<float, 5, NN>(h)) \
+                             : (ms == 3 ? setup_fast_row<double, 3, NN>(h) : setup_fast_row<double, 5, NN>(h))
+        FAST_SWITCH(p.nx, SETR)
+#undef SETR
+        if (g > 0) { h->fast_row = true; h->fast_row_grid = g; }
+    }
+    for (int a = 1; a < p.dim; ++a) {
+        if (!allow_fast_col || !fast_size(ns[a])) continue;
+        const int ntl = (p.nx / (h->fp32 ? 4 : 2)) * (p.dim == 2 ? 1 : (a == 1 ? p.nz : p.ny));
+        int g = 0;
+#define SETC(NN) g = h->fp32 ? (ms == 3 ? setup_fast_col<float, 3, NN>(h, ntl) : setup_fast_col<float, 5, NN>(h, ntl)) \
+                             : (ms == 3 ? setup_fast_col<double, 3, NN>(h, ntl) : setup_fast_col<double, 5, NN>(h, ntl))
+        FAST_SWITCH(ns[a], SETC)
+#undef SETC
+        if (g > 0) { h->fast_col[a] = true; h->fast_col_grid[a] = g; }
+    }
+    cudaGetLastError();   // clear any attribute/occupancy probe error
     h->obsl.grid = dim3((unsigned)((h->npts + 255) / 256));
     const size_t nq = 3 * ms + 3;
-    const size_t npart = std::max<size_t>((size_t)h->obsl.grid.x * nq, (size_t)h->row.grid.x * ms) + 64;
+    const size_t npart = std::max<size_t>((size_t)h->obsl.grid.x * nq, (size_t)std::max<int>(h->row.grid.x, h->fast_row_grid) * ms) + 64;
     CK(cudaMalloc(&h->part, npart * sizeof(double)));
     CK(cudaMalloc(&h->info, 4 * INFO_LEN * sizeof(double)));
     h->info_prev = h->info + INFO_LEN;
@@ -839,6 +943,16 @@ int fgpe_profile_read(fgpe_t* h, double* ms, long long* n, int reset) {
     }
     return FGPE_OK;
 }
+
+#ifdef FGPE_CHECK_ALIGN
+// Diagnostic builds only (not part of the ABI).
+int fgpe_debug_align_fault(unsigned long long* out4) {
+    fgpe_t* h = nullptr;
+    CK(cudaDeviceSynchronize());
+    CK(cudaMemcpyFromSymbol(out4, g_align_fault, 4 * sizeof(unsigned long long)));
+    return FGPE_OK;
+}
+#endif
 
 int fgpe_kernel_launches(fgpe_t* h, long long* count) {
     if (!h || !count) return fail(h, FGPE_E_ARG, "null argument");

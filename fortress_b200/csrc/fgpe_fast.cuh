@@ -1,0 +1,318 @@
+// fgpe_fast.cuh -- compile-time specialised, persistent row/column kernels.
+//
+// Same algorithm and data layout as the generic kernels (in-place DIF
+// forward / DIT inverse transforms, digit-reversed spectra, padded shared
+// tiles), but the line length N, the tile shape and the block size are
+// template constants, so all index arithmetic folds to shifts and the
+// butterfly loops unroll.  Each block is persistent over tiles and
+// double-buffers them: while tile i is transformed, tile i+1 streams into the
+// other shared buffer with cp.async (16-byte chunks, padded destination), so
+// HBM traffic overlaps the FP64/FP32 work.
+#pragma once
+#include "fgpe_device.cuh"
+#include "fgpe_kernels.h"
+
+namespace fgpe {
+
+struct CPlan {
+    int nf;
+    int r[12];
+};
+constexpr CPlan cplan(int n) {
+    CPlan p{0, {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0}};
+    while (n % 8 == 0) { p.r[p.nf++] = 8; n /= 8; }
+    if (n % 4 == 0) { p.r[p.nf++] = 4; n /= 4; }
+    if (n % 2 == 0) { p.r[p.nf++] = 2; n /= 2; }
+    while (n % 3 == 0) { p.r[p.nf++] = 3; n /= 3; }
+    while (n % 5 == 0) { p.r[p.nf++] = 5; n /= 5; }
+    return p;
+}
+constexpr int cplan_block(int n, int pass) {
+    CPlan pl = cplan(n);
+    int b = n;
+    for (int i = 0; i < pass; ++i) b /= pl.r[i];
+    return b;
+}
+constexpr int cpad(int n) { return n + (n + 7) / 8; }
+
+// ------------------------------------------------------------ line maps
+template <int N, int NL> struct RowTile {
+    static constexpr int LP = cpad(N);
+    static __device__ __forceinline__ void split(int b, int nb, int& l, int& q) { l = b / nb; q = b - l * nb; }
+    static __device__ __forceinline__ int at(int l, int e) { return l * LP + e + (e >> 3); }
+};
+template <int N, int TX> struct ColTile {
+    static constexpr int LPN = cpad(N);
+    static __device__ __forceinline__ void split(int b, int nb, int& l, int& q) {
+        const int t = b % TX; const int w = b / TX; q = w % nb; const int m = w / nb; l = m * TX + t;
+    }
+    static __device__ __forceinline__ int at(int l, int e) { return ((l / TX) * LPN + e + (e >> 3)) * TX + (l % TX); }
+};
+
+template <typename T, bool INV, int N, int NL, int TH, int P, class Map>
+__device__ __forceinline__ void ct_pass(cx<T>* s, const cx<T>* __restrict__ tw) {
+    constexpr CPlan pl = cplan(N);
+    constexpr int R = pl.r[P];
+    constexpr int BP = cplan_block(N, P);
+    constexpr int SI = BP / R, NB = N / R, TOT = NL * NB, ITER = (TOT + TH - 1) / TH, TSTEP = N / BP;
+#pragma unroll
+    for (int it = 0; it < ITER; ++it) {
+        const int b = threadIdx.x + it * TH;
+        if ((TOT % TH) == 0 || b < TOT) {
+            int l, q; Map::split(b, NB, l, q);
+            const int blk = q / SI, n2 = q - blk * SI;
+            const int e0 = blk * BP + n2;
+            cx<T> v[R];
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[r] = s[Map::at(l, e0 + r * SI)];
+            if (!INV) {
+                Dft<T, false, R>::run(v);
+                if (SI > 1 && n2) {
+#pragma unroll
+                    for (int r = 1; r < R; ++r) v[r] = cmul(v[r], tw[n2 * r * TSTEP]);
+                }
+            } else {
+                if (SI > 1 && n2) {
+#pragma unroll
+                    for (int r = 1; r < R; ++r) v[r] = cmulc(v[r], tw[n2 * r * TSTEP]);
+                }
+                Dft<T, true, R>::run(v);
+            }
+#pragma unroll
+            for (int r = 0; r < R; ++r) s[Map::at(l, e0 + r * SI)] = v[r];
+        }
+    }
+    __syncthreads();
+}
+
+template <typename T, bool INV, int N, int NL, int TH, class Map, int P = 0>
+__device__ __forceinline__ void ct_fft(cx<T>* s, const cx<T>* __restrict__ tw) {
+    constexpr CPlan pl = cplan(N);
+    if constexpr (P < pl.nf) {
+        constexpr int PP = INV ? pl.nf - 1 - P : P;
+        ct_pass<T, INV, N, NL, TH, PP, Map>(s, tw);
+        ct_fft<T, INV, N, NL, TH, Map, P + 1>(s, tw);
+    }
+}
+
+// ------------------------------------------------------------- cp.async
+#ifdef FGPE_CHECK_ALIGN
+// Diagnostic build only: record the first misaligned copy and skip it.
+__device__ unsigned long long g_align_fault[4];
+__device__ __forceinline__ bool align_bad(const void* s, const void* g, unsigned bytes, int site) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(s);
+    if ((d % bytes) == 0 && ((unsigned long long)g % bytes) == 0) return false;
+    if (atomicCAS(&g_align_fault[0], 0ull, 1ull) == 0ull) {
+        g_align_fault[1] = (unsigned long long)site;
+        g_align_fault[2] = d;
+        g_align_fault[3] = (unsigned long long)g;
+    }
+    return true;
+}
+#define FGPE_ALIGN_GUARD(s, g, b, site) if (align_bad(s, g, b, site)) return
+#else
+#define FGPE_ALIGN_GUARD(s, g, b, site)
+#endif
+
+__device__ __forceinline__ void cp16(void* smem_dst, const void* gsrc) {
+    FGPE_ALIGN_GUARD(smem_dst, gsrc, 16, 16);
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp8(void* smem_dst, const void* gsrc) {
+    FGPE_ALIGN_GUARD(smem_dst, gsrc, 8, 8);
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(gsrc) : "memory");
+}
+// One complex element: 16-byte copy for complex128, 8-byte for complex64 (the
+// padded row layout puts complex64 elements on 8-byte boundaries only).
+template <typename T> __device__ __forceinline__ void cp_elem(cx<T>* smem_dst, const cx<T>* gsrc) {
+    if constexpr (sizeof(cx<T>) == 16) cp16(smem_dst, gsrc);
+    else cp8(smem_dst, gsrc);
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// ------------------------------------------------------------ row kernel
+// Tiles of R x-lines (all MS components); see k_row for the three modes.
+template <typename T, int MS, int N, int R, int TH>
+__global__ void __launch_bounds__(TH, 1) k_row_fast(StepConst c, RowArgs a) {
+    using RT = RowTile<N, MS * R>;
+    constexpr int LP = RT::LP;
+    constexpr int TILE = MS * R * LP;
+    constexpr int NCH = MS * R * N;                    // one async copy per element
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cx<T>* bufs = (cx<T>*)smraw;
+    __shared__ double red[32 * (MS + 1)];
+    __shared__ double bsum[MS];
+    const long long np = c.npts;
+    const int ntiles = (c.ny * c.nz) / R;
+    const cx<T>* twx = (const cx<T>*)c.twx;
+    const cx<T>* src = (a.mode == ROW_FWD) ? (const cx<T>*)a.psi : (const cx<T>*)a.S;
+    cx<T>* S = (cx<T>*)a.S;
+    cx<T>* snap = (cx<T>*)a.snap;
+
+    auto issue = [&](int tile, cx<T>* dst) {
+        const int row0 = tile * R;
+        for (int ch = threadIdx.x; ch < NCH; ch += TH) {
+            const int x = ch % N;
+            const int q = ch / N;
+            const int r = q % R, m = q / R;
+            cp_elem<T>(dst + (m * R + r) * LP + x + (x >> 3), src + (size_t)m * np + (size_t)(row0 + r) * N + x);
+        }
+    };
+
+    double acc[MS];
+#pragma unroll
+    for (int m = 0; m < MS; ++m) acc[m] = 0.0;
+    int tile = blockIdx.x;
+    if (tile < ntiles) issue(tile, bufs);
+    cp_commit();
+    for (int it = 0; tile < ntiles; ++it, tile += gridDim.x) {
+        cx<T>* cur = bufs + (it & 1) * TILE;
+        const int nt = tile + gridDim.x;
+        if (nt < ntiles) issue(nt, bufs + ((it + 1) & 1) * TILE);
+        cp_commit();
+        cp_wait<1>();
+        __syncthreads();
+        const int row0 = tile * R;
+        if (a.mode == ROW_FWD) {
+            ct_fft<T, false, N, MS * R, TH, RT>(cur, twx);
+        } else {
+            ct_fft<T, true, N, MS * R, TH, RT>(cur, twx);
+            if (a.mode == ROW_INV) {
+                const T inv = (T)(1.0 / N);
+                cx<T>* dst = (cx<T>*)a.psi;
+                for (int idx = threadIdx.x; idx < MS * R * N; idx += TH) {
+                    const int x = idx % N, q = idx / N, r = q % R, m = q / R;
+                    dst[(size_t)m * np + (size_t)(row0 + r) * N + x] = cscale(cur[(m * R + r) * LP + x + (x >> 3)], inv);
+                }
+                __syncthreads();
+                continue;
+            }
+            for (int p = threadIdx.x; p < R * N; p += TH) {
+                const int x = p % N, r = p / N;
+                const int row = row0 + r;
+                const int j = row % c.ny, k = row / c.ny;
+                cx<T> v[MS];
+#pragma unroll
+                for (int m = 0; m < MS; ++m) v[m] = cur[(m * R + r) * LP + x + (x >> 3)];
+                double V = c.vx[x];
+                if (c.dim >= 2) V += c.vy[j];
+                if (c.dim >= 3) V += c.vz[k];
+                apply_se<T, MS>(c, v);
+                apply_sp<T, MS>(c, (T)V, v);
+                double w = c.wx[x];
+                if (c.dim >= 2) w *= c.wy[j];
+                if (c.dim >= 3) w *= c.wz[k];
+#pragma unroll
+                for (int m = 0; m < MS; ++m) {
+                    acc[m] += w * ((double)v[m].x * (double)v[m].x + (double)v[m].y * (double)v[m].y);
+                    cur[(m * R + r) * LP + x + (x >> 3)] = v[m];
+                }
+                if (snap) {
+#pragma unroll
+                    for (int m = 0; m < MS; ++m) snap[(size_t)m * np + (size_t)row * N + x] = v[m];
+                }
+            }
+            __syncthreads();
+            ct_fft<T, false, N, MS * R, TH, RT>(cur, twx);
+        }
+        for (int idx = threadIdx.x; idx < MS * R * N; idx += TH) {
+            const int x = idx % N, q = idx / N, r = q % R, m = q / R;
+            S[(size_t)m * np + (size_t)(row0 + r) * N + x] = cur[(m * R + r) * LP + x + (x >> 3)];
+        }
+        __syncthreads();
+    }
+    cp_wait<0>();
+    if (a.mode != ROW_FULL) return;
+    block_sum<MS>(acc, red, bsum);
+    if (threadIdx.x < MS) a.part[(size_t)blockIdx.x * MS + threadIdx.x] = bsum[threadIdx.x];
+    finish_norms<MS>(c, a.part, a.counter, a.info, red);
+}
+
+// --------------------------------------------------------- column kernel
+// Tiles of TX adjacent x positions, full lines of N along the transformed
+// axis; persistent over (x-tile, other) pairs.
+template <typename T, int MS, int N, int TX, int TH>
+__global__ void __launch_bounds__(TH, 1) k_col_fast(StepConst c, ColArgs a) {
+    using CT = ColTile<N, TX>;
+    constexpr int LPN = CT::LPN;
+    constexpr int TILE = MS * LPN * TX;
+    constexpr int EPC = 16 / (int)sizeof(cx<T>);
+    // every 16-byte chunk starts at a multiple of EPC elements of a tile row
+    // of TX elements: destinations stay 16-byte aligned
+    static_assert(TX % EPC == 0, "column tile narrower than a 16-byte chunk");
+    constexpr int CPL = TX / EPC;                      // chunks per (m, e)
+    constexpr int NCH = MS * N * CPL;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cx<T>* bufs = (cx<T>*)smraw;
+    const long long np = c.npts;
+    const int nxt = c.nx / TX;
+    const int nother = (int)a.n_other;
+    const int ntiles = nxt * nother;
+    const cx<T>* tw = (const cx<T>*)a.tw;
+    cx<T>* S = (cx<T>*)a.S;
+    T fac = (T)1;
+    if (a.flags & COL_SCALE) fac = (T)(a.info[INFO_SCALE] * a.cfac);
+
+    auto issue = [&](int tile, cx<T>* dst) {
+        const int x0 = (tile % nxt) * TX;
+        const long long off = (long long)(tile / nxt) * a.other_stride + x0;
+        for (int ch = threadIdx.x; ch < NCH; ch += TH) {
+            const int tc = (ch % CPL) * EPC;
+            const int q = ch / CPL;
+            const int e = q % N, m = q / N;
+            cp16(dst + (m * LPN + e + (e >> 3)) * TX + tc, S + (size_t)m * np + off + (size_t)e * a.axis_stride + tc);
+        }
+    };
+
+    int tile = blockIdx.x;
+    if (tile < ntiles) issue(tile, bufs);
+    cp_commit();
+    for (int it = 0; tile < ntiles; ++it, tile += gridDim.x) {
+        cx<T>* cur = bufs + (it & 1) * TILE;
+        const int nt = tile + gridDim.x;
+        if (nt < ntiles) issue(nt, bufs + ((it + 1) & 1) * TILE);
+        cp_commit();
+        cp_wait<1>();
+        __syncthreads();
+        const int x0 = (tile % nxt) * TX;
+        const int oth = tile / nxt;
+        const long long off = (long long)oth * a.other_stride + x0;
+        if (a.flags & COL_SCALE) {
+            for (int idx = threadIdx.x; idx < MS * N * TX; idx += TH) {
+                const int t = idx % TX, q = idx / TX, e = q % N, m = q / N;
+                cx<T>& v = cur[(m * LPN + e + (e >> 3)) * TX + t];
+                v = cscale(v, fac);
+            }
+            __syncthreads();
+        }
+        if (a.flags & COL_FWD) ct_fft<T, false, N, MS * TX, TH, CT>(cur, tw);
+        if (a.flags & COL_KOP) {
+            for (int p = threadIdx.x; p < N * TX; p += TH) {
+                const int t = p % TX, e = p / TX;
+                const int ix = c.fx[x0 + t];
+                int iy, iz;
+                if (c.dim == 2) { iy = c.fy[e]; iz = 0; } else { iy = c.fy[oth]; iz = c.fz[e]; }
+                cx<T> v[MS];
+#pragma unroll
+                for (int m = 0; m < MS; ++m) v[m] = cur[(m * LPN + e + (e >> 3)) * TX + t];
+                apply_ke<T, MS>(c, ix, iy, iz, v);
+                apply_soc<T, MS>(c, c.kx[ix], c.dim >= 2 ? c.ky[iy] : 0.0, v);
+#pragma unroll
+                for (int m = 0; m < MS; ++m) cur[(m * LPN + e + (e >> 3)) * TX + t] = v[m];
+            }
+            __syncthreads();
+        }
+        if (a.flags & COL_INV) ct_fft<T, true, N, MS * TX, TH, CT>(cur, tw);
+        for (int idx = threadIdx.x; idx < MS * N * TX; idx += TH) {
+            const int t = idx % TX, q = idx / TX, e = q % N, m = q / N;
+            S[(size_t)m * np + off + (size_t)e * a.axis_stride + t] = cur[(m * LPN + e + (e >> 3)) * TX + t];
+        }
+        __syncthreads();
+    }
+    cp_wait<0>();
+}
+
+}  // namespace fgpe

@@ -43,6 +43,7 @@ struct ColArgs {
     double cfac;       // 1/(NX*NY*NZ) folded into the scale on load
     long long axis_stride, other_stride;
     int n, tx, flags;
+    int n_other;       // number of positions along the third axis (1 in 2D)
 };
 
 struct OneDArgs {

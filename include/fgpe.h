@@ -39,6 +39,8 @@ enum {
 };
 
 enum { FGPE_FP64 = 0, FGPE_FP32 = 1 };
+enum { FGPE_KERNELS_AUTO = 0, FGPE_KERNELS_GENERIC = 1,
+       FGPE_KERNELS_FAST_ROW_ONLY = 2, FGPE_KERNELS_FAST_COL_ONLY = 3 };
 
 /* Step flags for fgpe_step_ex. */
 enum {
@@ -62,7 +64,10 @@ typedef struct fgpe_params {
     double alpha[3];    /* ALPHAX, ALPHAY, ALPHAZ = NU{X,Y,Z}/NUX */
     int precision;      /* FGPE_FP64 or FGPE_FP32 (FP32 FFTs/exponentials,
                            FP64 reductions and renormalisation) */
-    int reserved[7];
+    int kernels;        /* FGPE_KERNELS_AUTO: size-specialised persistent
+                           kernels where compiled, else generic;
+                           FGPE_KERNELS_GENERIC: generic kernels only */
+    int reserved[6];
 } fgpe_params;
 
 typedef struct fgpe_s fgpe_t;

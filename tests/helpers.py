@@ -43,3 +43,10 @@ def initial_state(orc, seed=0):
 
 def rel_err(a, b):
     return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+# Grids whose lines hit the size-specialised persistent kernels (128, 192,
+# 256, 384, 512) on some axes and the generic ones on others.
+FAST_CASES = [
+    (2, 2, 1, (128, 192)), (2, 2, 0, (256, 128)), (2, 1, 1, (384, 128)), (2, 1, 0, (512, 96)),
+    (3, 1, 1, (128, 128, 16)), (3, 2, 0, (16, 128, 128)), (3, 1, 0, (192, 16, 256)),
+]

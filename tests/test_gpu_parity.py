@@ -85,3 +85,49 @@ def test_error_paths(F):
     p = F.Propagator(dim=2, spin=1, n=(32, 32), d=(0.1, 0.1), dt=1e-3, imag_time=1, tau=(1, 0, 0))
     with pytest.raises(F.FgpeError):
         p.step(1)      # no state set
+
+
+from tests.helpers import FAST_CASES  # noqa: E402
+
+
+@pytest.mark.parametrize("case", FAST_CASES, ids=case_id)
+def test_fast_kernels(F, case):
+    orc, prop = _pair(F, case, seed=3)
+    dim, spin, imag, n = case
+    if imag:
+        orc.normt(); prop.normt()
+    norm_o = orc.step(3)
+    prop.step(3)
+    assert rel_err(prop.state(), orc.state()) < 1e-11
+    assert np.allclose(prop.normc(), norm_o, rtol=1e-11, atol=0)
+    en_g = prop.observables()[0]
+    en_o = orc.energy()[0]
+    assert abs(en_g - en_o) <= 1e-10 * abs(en_o)
+
+
+@pytest.mark.parametrize("case", [FAST_CASES[0], FAST_CASES[4]], ids=case_id)
+def test_fast_kernels_fp32(F, case):
+    orc, prop = _pair(F, case, precision="fp32", seed=4)
+    dim, spin, imag, n = case
+    if imag:
+        orc.normt(); prop.normt()
+    orc.step(3)
+    prop.step(3)
+    assert rel_err(prop.state(), orc.state()) < 2e-5
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_fast_matches_generic_512(F, precision):
+    """Size-specialised and generic kernels agree on the 512^2 spin-2
+    real-time bench workload (GPU only, 20 steps)."""
+    p = case_params((2, 2, 0, (512, 512)))
+    rng = np.random.default_rng(5)
+    x = (np.arange(512) - 256) * p["d"][0]
+    g = np.exp(-(x[:, None] ** 2 + x[None, :] ** 2) / 8.0)
+    phi = np.stack([g * np.exp(1j * rng.uniform(-0.3, 0.3, g.shape)) for _ in range(5)], axis=-1)
+    a = F.Propagator(**p, precision=precision)
+    b = F.Propagator(**p, precision=precision, kernels="generic")
+    a.set_state(phi); b.set_state(phi)
+    a.step(20); b.step(20)
+    tol = 1e-12 if precision == "fp64" else 1e-5
+    assert rel_err(a.state(), b.state()) < tol
