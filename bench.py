@@ -286,7 +286,9 @@ def main():
     e2e_ms = ev[0].elapsed_time(ev[1]) + ev[2 * args.steps + 2].elapsed_time(ev[2 * args.steps + 3])
     e2e_ms += sum(ev[2 + 2 * k].elapsed_time(ev[3 + 2 * k]) for k in range(args.steps))
     norms = norms_host.numpy().reshape(args.steps, ms_comp)
-    assert np.all(np.isfinite(norms)) and abs(norms[-1].sum() - norms[0].sum()) < 1e-6 * norms[0].sum()
+    # real time conserves the norm (to rounding of the bulk precision)
+    drift_tol = 1e-6 if args.precision == "fp64" else 1e-3
+    assert np.all(np.isfinite(norms)) and abs(norms[-1].sum() - norms[0].sum()) < drift_tol * norms[0].sum()
     if dist:
         t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)

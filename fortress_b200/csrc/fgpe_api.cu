@@ -153,7 +153,10 @@ template <typename T, int MS> cudaError_t set_smem_attrs() {
 // kernels (same layout and results).
 constexpr int kFastN[] = {128, 192, 256, 384, 512};
 
-template <typename T> constexpr int col_tx() { return sizeof(T) == 8 ? 2 : 4; }
+#ifndef FGPE_COL_TX32
+#define FGPE_COL_TX32 2
+#endif
+template <typename T> constexpr int col_tx() { return sizeof(T) == 8 ? 2 : FGPE_COL_TX32; }
 constexpr int row_r(int n) { return n >= 384 ? 1 : 512 / n; }
 constexpr int fast_threads(int tot) {
     const int iter = (tot + 511) / 512;
@@ -162,8 +165,12 @@ constexpr int fast_threads(int tot) {
 }
 template <typename T, int MS, int N> constexpr int row_th() { return fast_threads(MS * row_r(N) * N / 8); }
 template <typename T, int MS, int N> constexpr int col_th() { return fast_threads(MS * col_tx<T>() * N / 8); }
-template <typename T, int MS, int N> constexpr size_t row_smem() { return 2ull * MS * row_r(N) * cpad(N) * sizeof(cx<T>); }
-template <typename T, int MS, int N> constexpr size_t col_smem() { return 2ull * MS * cpad(N) * col_tx<T>() * sizeof(cx<T>); }
+template <typename T, int MS, int N> constexpr size_t row_smem() {
+    return ((size_t)FGPE_ROW_NBUF * MS * row_r(N) * cpad(N) + (FGPE_TW_SMEM ? N : 0)) * sizeof(cx<T>);
+}
+template <typename T, int MS, int N> constexpr size_t col_smem() {
+    return ((size_t)FGPE_COL_NBUF * MS * cpad(N) * col_tx<T>() + (FGPE_TW_SMEM ? N : 0)) * sizeof(cx<T>);
+}
 
 template <class K> int grid_for(K kern, int th, size_t smem, int ntiles) {
     int dev = 0, nsm = 0, per = 0;
@@ -601,7 +608,7 @@ int fgpe_create(const fgpe_params* pin, fgpe_t** out) {
     }
     for (int a = 1; a < p.dim; ++a) {
         if (!allow_fast_col || !fast_size(ns[a])) continue;
-        const int ntl = (p.nx / (h->fp32 ? 4 : 2)) * (p.dim == 2 ? 1 : (a == 1 ? p.nz : p.ny));
+        const int ntl = (p.nx / (h->fp32 ? col_tx<float>() : col_tx<double>())) * (p.dim == 2 ? 1 : (a == 1 ? p.nz : p.ny));
         int g = 0;
 #define SETC(NN) g = h->fp32 ? (ms == 3 ? setup_fast_col<float, 3, NN>(h, ntl) : setup_fast_col<float, 5, NN>(h, ntl)) \
                              : (ms == 3 ? setup_fast_col<double, 3, NN>(h, ntl) : setup_fast_col<double, 5, NN>(h, ntl))

@@ -299,7 +299,8 @@ __device__ __forceinline__ void apply_soc(const StepConst& c, double kx, double 
     }
     // u_L *= exp(-i CDT L alpha)
     const cx<T> l1 = cdt_phase<T>(c.imag, (T)c.dt, (T)alpha);
-    const cx<T> lm1 = cdt_phase<T>(c.imag, (T)c.dt, (T)(-alpha));
+    // real time: exp(+i dt alpha) = conj; imaginary time: exp(+dt alpha)
+    const cx<T> lm1 = c.imag ? mk<T>(exp_t((T)(c.dt * alpha)), (T)0) : cconj(l1);
 #pragma unroll
     for (int m = 0; m < MS; ++m) {
         const int L = m - S;
@@ -411,23 +412,30 @@ __device__ __forceinline__ void se_spin2(const StepConst& c, cx<T>* v) {
     if (nrm > (T)0.5) nsub = (int)ceil(nrm / (T)0.5);
     if (nsub > 4096) nsub = 4096;
     const T h = dt / (T)nsub;  // z = -i h (real) or -h (imag)
+    const T hn = nrm / (T)nsub;
+    // Number of Taylor terms fixed beforehand: the remainder after K terms is
+    // below hn^(K+1)/(K+1)! * e^hn relative to |v|, and |y| >= e^-hn |v|
+    // (e^{-h H} can contract by at most e^-hn), so stop once
+    // hn^(K+1)/(K+1)! * e^(2 hn) <= eps.  hn <= 1/2 keeps K <= 18 in FP64.
+    int K = 1;
+    {
+        const T e2 = exp_t((T)2 * hn);
+        T bnd = hn * hn * (T)0.5;
+        while (bnd * e2 > Eps<T>::v() * (T)0.5 && K < 40) { ++K; bnd *= hn / (T)(K + 1); }
+    }
     for (int sidx = 0; sidx < nsub; ++sidx) {
         cx<T> term[5], y[5];
 #pragma unroll
         for (int m = 0; m < 5; ++m) { term[m] = v[m]; y[m] = v[m]; }
-        for (int k = 1; k <= 40; ++k) {
+        for (int k = 1; k <= K; ++k) {
             hmul<T>(ca, term, hv);
             const T f = h / (T)k;
-            T tmax = 0, ymax = 0;
 #pragma unroll
             for (int m = 0; m < 5; ++m) {
                 if (c.imag) term[m] = mk<T>(-f * hv[m].x, -f * hv[m].y);
                 else term[m] = mk<T>(f * hv[m].y, -f * hv[m].x);
                 y[m] = cadd(y[m], term[m]);
-                tmax = fmax(tmax, fabs(term[m].x) + fabs(term[m].y));
-                ymax = fmax(ymax, fabs(y[m].x) + fabs(y[m].y));
             }
-            if (tmax <= Eps<T>::v() * (T)0.25 * ymax) break;
         }
 #pragma unroll
         for (int m = 0; m < 5; ++m) v[m] = y[m];
@@ -470,28 +478,55 @@ __device__ __forceinline__ void se_spin1(const StepConst& c, cx<T>* v) {
     v[2] = cadd(p3, cadd(cscale(u3, dc), w3));
 }
 
+// exp(-i CDT x) for |dt x| <= 1/16 by the Taylor series of sin/cos (real
+// time) or exp (imaginary time) truncated after the x^10 term: the first
+// omitted term is below (1/16)^11/11! ~ 8e-22, under FP64 rounding.
+template <typename T> __device__ __forceinline__ cx<T> small_phase(int imag, T th) {
+    const T t2 = th * th;
+    if (imag) {
+        // exp(-th) = sum (-th)^k/k!
+        const T e = (T)1 - th * ((T)1 - th * ((T)(1.0 / 2) - th * ((T)(1.0 / 6) - th * ((T)(1.0 / 24) - th * ((T)(1.0 / 120)
+                    - th * ((T)(1.0 / 720) - th * ((T)(1.0 / 5040) - th * ((T)(1.0 / 40320) - th * ((T)(1.0 / 362880)
+                    - th * (T)(1.0 / 3628800))))))))));
+        return mk<T>(e, (T)0);
+    }
+    const T cs = (T)1 - t2 * ((T)(1.0 / 2) - t2 * ((T)(1.0 / 24) - t2 * ((T)(1.0 / 720) - t2 * ((T)(1.0 / 40320)
+                 - t2 * (T)(1.0 / 3628800)))));
+    const T sn = th * ((T)1 - t2 * ((T)(1.0 / 6) - t2 * ((T)(1.0 / 120) - t2 * ((T)(1.0 / 5040) - t2 * (T)(1.0 / 362880)))));
+    return mk<T>(cs, -sn);
+}
+
 // SP (cgpe1d.f90:847-896): phi_m <- phi_m exp(-i CDT T_m), densities after SE.
+// T_m = A + B_m with the common part A = V + tau0 rho; exp(-i CDT A) is
+// computed once and the component parts B_m (tau1/tau2 terms, small for
+// physical states) by small_phase when |dt B_m| <= 1/16.
 template <typename T, int MS>
 __device__ __forceinline__ void apply_sp(const StepConst& c, T V, cx<T>* v) {
     const T t0 = (T)c.tau0, t1 = (T)c.tau1, t2 = (T)c.tau2;
     T a[MS], rho = 0;
 #pragma unroll
     for (int m = 0; m < MS; ++m) { a[m] = cabs2(v[m]); rho += a[m]; }
-    T Tm[MS];
+    T B[MS];
     if constexpr (MS == 3) {
-        Tm[0] = V + t0 * rho + t1 * (a[0] + a[1] - a[2]);
-        Tm[1] = V + t0 * rho + t1 * (a[0] + a[2]);
-        Tm[2] = V + t0 * rho + t1 * (a[2] + a[1] - a[0]);
+        B[0] = t1 * (a[0] + a[1] - a[2]);
+        B[1] = t1 * (a[0] + a[2]);
+        B[2] = t1 * (a[2] + a[1] - a[0]);
     } else {
         const T fz = (T)2 * a[0] + a[1] - a[MS - 2] - (T)2 * a[MS - 1];
-        Tm[0] = V + t0 * rho + (T)2 * t1 * fz + (T)0.4 * t2 * a[MS - 1];
-        Tm[1] = V + t0 * rho + t1 * fz + (T)0.4 * t2 * a[MS - 2];
-        Tm[2] = V + t0 * rho + (T)0.2 * t2 * a[2];
-        Tm[MS - 2] = V + t0 * rho - t1 * fz + (T)0.4 * t2 * a[1];
-        Tm[MS - 1] = V + t0 * rho - (T)2 * t1 * fz + (T)0.4 * t2 * a[0];
+        B[0] = (T)2 * t1 * fz + (T)0.4 * t2 * a[MS - 1];
+        B[1] = t1 * fz + (T)0.4 * t2 * a[MS - 2];
+        B[2] = (T)0.2 * t2 * a[2];
+        B[MS - 2] = -t1 * fz + (T)0.4 * t2 * a[1];
+        B[MS - 1] = (T)-2 * t1 * fz + (T)0.4 * t2 * a[0];
     }
+    const T dt = (T)c.dt;
+    const cx<T> eA = cdt_phase<T>(c.imag, dt, V + t0 * rho);
 #pragma unroll
-    for (int m = 0; m < MS; ++m) v[m] = cmul(v[m], cdt_phase<T>(c.imag, (T)c.dt, Tm[m]));
+    for (int m = 0; m < MS; ++m) {
+        const T th = dt * B[m];
+        const cx<T> eB = fabs(th) <= (T)0.0625 ? small_phase<T>(c.imag, th) : cdt_phase<T>(c.imag, dt, B[m]);
+        v[m] = cmul(v[m], cmul(eA, eB));
+    }
 }
 
 template <typename T, int MS>

@@ -133,10 +133,28 @@ template <typename T> __device__ __forceinline__ void cp_elem(cx<T>* smem_dst, c
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N> __device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
+// Blocks per SM the launch bounds target and shared buffers per block
+// (2 = double-buffered prefetch).
+#ifndef FGPE_ROW_MINB
+#define FGPE_ROW_MINB 2
+#endif
+#ifndef FGPE_ROW_NBUF
+#define FGPE_ROW_NBUF 2
+#endif
+#ifndef FGPE_COL_MINB
+#define FGPE_COL_MINB 2
+#endif
+#ifndef FGPE_COL_NBUF
+#define FGPE_COL_NBUF 1
+#endif
+#ifndef FGPE_TW_SMEM
+#define FGPE_TW_SMEM 1
+#endif
+
 // ------------------------------------------------------------ row kernel
 // Tiles of R x-lines (all MS components); see k_row for the three modes.
-template <typename T, int MS, int N, int R, int TH>
-__global__ void __launch_bounds__(TH, 1) k_row_fast(StepConst c, RowArgs a) {
+template <typename T, int MS, int N, int R, int TH, int NBUF = FGPE_ROW_NBUF>
+__global__ void __launch_bounds__(TH, FGPE_ROW_MINB) k_row_fast(StepConst c, RowArgs a) {
     using RT = RowTile<N, MS * R>;
     constexpr int LP = RT::LP;
     constexpr int TILE = MS * R * LP;
@@ -148,6 +166,12 @@ __global__ void __launch_bounds__(TH, 1) k_row_fast(StepConst c, RowArgs a) {
     const long long np = c.npts;
     const int ntiles = (c.ny * c.nz) / R;
     const cx<T>* twx = (const cx<T>*)c.twx;
+    if (FGPE_TW_SMEM) {
+        // the twiddle table sits after the tile buffers
+        cx<T>* tws = bufs + NBUF * TILE;
+        for (int i = threadIdx.x; i < N; i += TH) tws[i] = twx[i];
+        twx = tws;   // made visible by the first barrier of the tile loop
+    }
     const cx<T>* src = (a.mode == ROW_FWD) ? (const cx<T>*)a.psi : (const cx<T>*)a.S;
     cx<T>* S = (cx<T>*)a.S;
     cx<T>* snap = (cx<T>*)a.snap;
@@ -166,14 +190,22 @@ __global__ void __launch_bounds__(TH, 1) k_row_fast(StepConst c, RowArgs a) {
 #pragma unroll
     for (int m = 0; m < MS; ++m) acc[m] = 0.0;
     int tile = blockIdx.x;
-    if (tile < ntiles) issue(tile, bufs);
-    cp_commit();
-    for (int it = 0; tile < ntiles; ++it, tile += gridDim.x) {
-        cx<T>* cur = bufs + (it & 1) * TILE;
-        const int nt = tile + gridDim.x;
-        if (nt < ntiles) issue(nt, bufs + ((it + 1) & 1) * TILE);
+    if (NBUF == 2) {
+        if (tile < ntiles) issue(tile, bufs);
         cp_commit();
-        cp_wait<1>();
+    }
+    for (int it = 0; tile < ntiles; ++it, tile += gridDim.x) {
+        cx<T>* cur = bufs + (NBUF == 2 ? (it & 1) * TILE : 0);
+        if (NBUF == 2) {
+            const int nt = tile + gridDim.x;
+            if (nt < ntiles) issue(nt, bufs + ((it + 1) & 1) * TILE);
+            cp_commit();
+            cp_wait<1>();
+        } else {
+            issue(tile, cur);
+            cp_commit();
+            cp_wait<0>();
+        }
         __syncthreads();
         const int row0 = tile * R;
         if (a.mode == ROW_FWD) {
@@ -234,8 +266,8 @@ __global__ void __launch_bounds__(TH, 1) k_row_fast(StepConst c, RowArgs a) {
 // --------------------------------------------------------- column kernel
 // Tiles of TX adjacent x positions, full lines of N along the transformed
 // axis; persistent over (x-tile, other) pairs.
-template <typename T, int MS, int N, int TX, int TH>
-__global__ void __launch_bounds__(TH, 1) k_col_fast(StepConst c, ColArgs a) {
+template <typename T, int MS, int N, int TX, int TH, int NBUF = FGPE_COL_NBUF>
+__global__ void __launch_bounds__(TH, FGPE_COL_MINB) k_col_fast(StepConst c, ColArgs a) {
     using CT = ColTile<N, TX>;
     constexpr int LPN = CT::LPN;
     constexpr int TILE = MS * LPN * TX;
@@ -252,6 +284,11 @@ __global__ void __launch_bounds__(TH, 1) k_col_fast(StepConst c, ColArgs a) {
     const int nother = (int)a.n_other;
     const int ntiles = nxt * nother;
     const cx<T>* tw = (const cx<T>*)a.tw;
+    if (FGPE_TW_SMEM) {
+        cx<T>* tws = bufs + NBUF * TILE;
+        for (int i = threadIdx.x; i < N; i += TH) tws[i] = tw[i];
+        tw = tws;
+    }
     cx<T>* S = (cx<T>*)a.S;
     T fac = (T)1;
     if (a.flags & COL_SCALE) fac = (T)(a.info[INFO_SCALE] * a.cfac);
@@ -268,14 +305,22 @@ __global__ void __launch_bounds__(TH, 1) k_col_fast(StepConst c, ColArgs a) {
     };
 
     int tile = blockIdx.x;
-    if (tile < ntiles) issue(tile, bufs);
-    cp_commit();
-    for (int it = 0; tile < ntiles; ++it, tile += gridDim.x) {
-        cx<T>* cur = bufs + (it & 1) * TILE;
-        const int nt = tile + gridDim.x;
-        if (nt < ntiles) issue(nt, bufs + ((it + 1) & 1) * TILE);
+    if (NBUF == 2) {
+        if (tile < ntiles) issue(tile, bufs);
         cp_commit();
-        cp_wait<1>();
+    }
+    for (int it = 0; tile < ntiles; ++it, tile += gridDim.x) {
+        cx<T>* cur = bufs + (NBUF == 2 ? (it & 1) * TILE : 0);
+        if (NBUF == 2) {
+            const int nt = tile + gridDim.x;
+            if (nt < ntiles) issue(nt, bufs + ((it + 1) & 1) * TILE);
+            cp_commit();
+            cp_wait<1>();
+        } else {
+            issue(tile, cur);
+            cp_commit();
+            cp_wait<0>();
+        }
         __syncthreads();
         const int x0 = (tile % nxt) * TX;
         const int oth = tile / nxt;
