@@ -19,6 +19,7 @@ FGPE_E_ARG = -1
 FGPE_E_CUDA = -2
 FGPE_E_STATE = -3
 FGPE_E_NONFINITE = -4
+FGPE_E_NEWTON = -5
 
 FGPE_FP64 = 0
 FGPE_FP32 = 1
@@ -50,7 +51,7 @@ class Params(ctypes.Structure):
                 ("dt", ctypes.c_double), ("imag_time", ctypes.c_int),
                 ("tau", ctypes.c_double * 3), ("gamma", ctypes.c_double * 3),
                 ("alpha", ctypes.c_double * 3), ("precision", ctypes.c_int),
-                ("kernels", ctypes.c_int), ("reserved", ctypes.c_int * 6)]
+                ("kernels", ctypes.c_int), ("mag", ctypes.c_double), ("reserved", ctypes.c_int * 4)]
 
 
 _LIB = None

@@ -174,4 +174,4 @@ class RunConfig:
         """Keyword arguments for :class:`fortress_b200.Propagator`."""
         return dict(dim=self.dim, spin=self.spin, n=self.n[: self.dim], d=self.d[: self.dim],
                     dt=self.dt, imag_time=bool(self.switch_im), tau=self.tau(),
-                    gamma=self.gamma[: self.dim], alpha=self.alpha, precision=precision)
+                    gamma=self.gamma[: self.dim], alpha=self.alpha, precision=precision, mag=self.mag)

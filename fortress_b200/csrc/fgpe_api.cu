@@ -316,10 +316,9 @@ void launch_1d(fgpe_t* h, int nsteps, void* snap_prev) {
     } while (0)
 
 template <typename T>
-__global__ void k_export(const T* psi, double* out, long long n2, const double* info) {
-    const double s = info[INFO_SCALE];
+__global__ void k_export(const T* psi, double* out, long long n2, long long per2, const double* info) {
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n2; t += (long long)gridDim.x * blockDim.x)
-        out[t] = s * (double)psi[t];
+        out[t] = info[INFO_SC + t / per2] * (double)psi[t];
 }
 template <typename T>
 __global__ void k_import(const double* in, T* psi, long long n2) {
@@ -438,6 +437,12 @@ int fgpe_create(const fgpe_params* pin, fgpe_t** out) {
     c.gx = p.gamma[0]; c.gy = p.dim >= 2 ? p.gamma[1] : 0.0; c.gz = p.dim >= 3 ? p.gamma[2] : 0.0;
     c.se_half = (p.dim == 1 && p.spin == 2);
     c.se_ge = (p.dim == 1);
+    {
+        // cgpe1d.f90:250, 443-444: projection in imaginary time when no SOC
+        bool soc = fabs(p.gamma[0]) > 1e-40 || (p.dim >= 2 && fabs(p.gamma[1]) > 1e-40) || (p.dim >= 3 && fabs(p.gamma[2]) > 1e-40);
+        c.project = (p.imag_time && !soc) ? 1 : 0;
+        c.mag = p.mag;
+    }
     for (int a = 0; a < 3; ++a) {
         FftPlan* pl = a == 0 ? &c.px : a == 1 ? &c.py : &c.pz;
         if (!plan_fft(ns[a], pl)) {
@@ -628,7 +633,8 @@ int fgpe_create(const fgpe_params* pin, fgpe_t** out) {
     CK(cudaMemset(h->counters, 0, 4 * sizeof(unsigned)));
     CK(cudaMallocHost(&h->h_small, 64 * sizeof(double)));
     std::vector<double> info0(4 * INFO_LEN, 0.0);
-    info0[INFO_SCALE] = 1.0; info0[INFO_LEN + INFO_SCALE] = 1.0;
+    for (int m = 0; m < 5; ++m) { info0[INFO_SC + m] = 1.0; info0[INFO_LEN + INFO_SC + m] = 1.0; }
+    info0[INFO_SIG] = info0[INFO_SIG + 1] = 20.0;   // cgpe1d.f90:425-426
     CK(cudaMemcpy(h->info, info0.data(), info0.size() * sizeof(double), cudaMemcpyHostToDevice));
     {
         cudaError_t e1 = h->fp32 ? set_smem_attrs<float, 3>() : set_smem_attrs<double, 3>();
@@ -677,8 +683,9 @@ static int import_dev(fgpe_t* h, const void* src_dev) {
     } else {
         CK(cudaMemcpyAsync(h->psi, src_dev, (size_t)n2 * 8, cudaMemcpyDeviceToDevice, h->st));
     }
-    double one[INFO_LEN] = {0};
-    one[INFO_SCALE] = 1.0;   // pageable source: staged before the call returns
+    double one[INFO_LEN] = {0};   // pageable source: staged before the call returns
+    for (int m = 0; m < 5; ++m) one[INFO_SC + m] = 1.0;
+    one[INFO_SIG] = one[INFO_SIG + 1] = 20.0;
     CK(cudaMemcpyAsync(h->info, one, sizeof(one), cudaMemcpyHostToDevice, h->st));
     CK(cudaMemcpyAsync(h->info_prev, one, sizeof(one), cudaMemcpyHostToDevice, h->st));
     CK(cudaGetLastError());
@@ -696,7 +703,8 @@ int fgpe_set_state(fgpe_t* h, const double* phi) {
     }
     CK(cudaMemcpyAsync(h->psi, phi, bytes, cudaMemcpyHostToDevice, h->st));
     double one[INFO_LEN] = {0};
-    one[INFO_SCALE] = 1.0;
+    for (int m = 0; m < 5; ++m) one[INFO_SC + m] = 1.0;
+    one[INFO_SIG] = one[INFO_SIG + 1] = 20.0;
     CK(cudaMemcpyAsync(h->info, one, sizeof(one), cudaMemcpyHostToDevice, h->st));
     CK(cudaMemcpyAsync(h->info_prev, one, sizeof(one), cudaMemcpyHostToDevice, h->st));
     h->psi_valid = true; h->S_valid = false; h->prev_valid = false; h->norms_valid = false; h->has_state = true;
@@ -713,8 +721,8 @@ static int export_to(fgpe_t* h, void* dst, cudaMemcpyKind kind) {
     int r = materialize(h); if (r) return r;
     r = ensure_stage(h); if (r) return r;
     const long long n2 = h->npts * h->ms * 2;
-    if (h->fp32) k_export<float><<<148 * 8, 256, 0, h->st>>>((const float*)h->psi, (double*)h->stage, n2, h->info);
-    else k_export<double><<<148 * 8, 256, 0, h->st>>>((const double*)h->psi, (double*)h->stage, n2, h->info);
+    if (h->fp32) k_export<float><<<148 * 8, 256, 0, h->st>>>((const float*)h->psi, (double*)h->stage, n2, 2 * h->npts, h->info);
+    else k_export<double><<<148 * 8, 256, 0, h->st>>>((const double*)h->psi, (double*)h->stage, n2, 2 * h->npts, h->info);
     h->launches++;
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(dst, h->stage, (size_t)n2 * 8, kind, h->st));
@@ -817,6 +825,8 @@ int fgpe_norms(fgpe_t* h, double* norm) {
     if (h->norms_valid) {
         int r = sync_info_err(h, h->info); if (r) return r;
         for (int m = 0; m < h->ms; ++m) norm[m] = h->h_small[INFO_NORM + m];
+        if (h->h_small[INFO_ERR] == 2.0)
+            return fail(h, FGPE_E_NEWTON, "Newton-Raphson subroutine could not calculate the roots within 1e-6 tolerance");
         if (h->h_small[INFO_ERR] != 0.0) return fail(h, FGPE_E_NONFINITE, "non-finite norm in a step");
         return check_err(h);
     }
@@ -869,8 +879,8 @@ int fgpe_center(fgpe_t* h, double* out) {
         CK(cudaMemcpyAsync((char*)h->h_small + m * 16, (char*)h->psi + ((size_t)m * h->npts + idx) * h->cs, h->cs, cudaMemcpyDeviceToHost, h->st));
     CK(cudaMemcpyAsync(h->h_small + 32, h->info, INFO_LEN * sizeof(double), cudaMemcpyDeviceToHost, h->st));
     CK(cudaStreamSynchronize(h->st));
-    const double s = h->h_small[32 + INFO_SCALE];
     for (int m = 0; m < h->ms; ++m) {
+        const double s = h->h_small[32 + INFO_SC + m];
         double re, im;
         if (h->fp32) { float f[2]; memcpy(f, (char*)h->h_small + m * 16, 8); re = f[0]; im = f[1]; }
         else { memcpy(&re, (char*)h->h_small + m * 16, 8); memcpy(&im, (char*)h->h_small + m * 16 + 8, 8); }
@@ -884,11 +894,11 @@ int fgpe_apply_op(fgpe_t* h, int op) {
     if (!h->has_state) return fail(h, FGPE_E_STATE, "no state set");
     int r = materialize(h); if (r) return r;
     // fold the pending scale into psi
-    if (h->fp32) k_apply_scale<float><<<148 * 8, 256, 0, h->st>>>((float*)h->psi, h->npts * h->ms * 2, h->info);
-    else k_apply_scale<double><<<148 * 8, 256, 0, h->st>>>((double*)h->psi, h->npts * h->ms * 2, h->info);
+    if (h->fp32) k_apply_scale<float><<<148 * 8, 256, 0, h->st>>>((float*)h->psi, h->npts * h->ms * 2, 2 * h->npts, h->info);
+    else k_apply_scale<double><<<148 * 8, 256, 0, h->st>>>((double*)h->psi, h->npts * h->ms * 2, 2 * h->npts, h->info);
     h->launches++;
-    const double one = 1.0;   // pageable source: staged before the call returns
-    CK(cudaMemcpyAsync(h->info + INFO_SCALE, &one, sizeof(double), cudaMemcpyHostToDevice, h->st));
+    const double ones[5] = {1.0, 1.0, 1.0, 1.0, 1.0};   // pageable source: staged before the call returns
+    CK(cudaMemcpyAsync(h->info + INFO_SC, ones, sizeof(ones), cudaMemcpyHostToDevice, h->st));
     switch (op) {
         case FGPE_OP_FFT: {
             void* keep = h->S;

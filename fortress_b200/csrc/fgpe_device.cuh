@@ -226,6 +226,8 @@ struct StepConst {
     double gx, gy, gz;
     int se_half;              // 1D spin-2 predictor uses CDT/2 (cgpe1d.f90:1443)
     int se_ge;                // 1D spin-1 uses |OMEGA| >= EPS (cgpe1d.f90:1413)
+    int project;              // imaginary time without SOC: magnetisation projection
+    double mag;               // MAG of the projection
     const double *kx, *ky, *kz;
     const double *xg, *yg, *zg;
     const double *wx, *wy, *wz;     // Simpson weight vectors
@@ -533,6 +535,62 @@ template <typename T, int MS>
 __device__ __forceinline__ void apply_se(const StepConst& c, cx<T>* v) {
     if constexpr (MS == 3) se_spin1<T>(c, v);
     else se_spin2<T>(c, v);
+}
+
+// --------------------------------------------- renormalisation scales
+// After a step's NORMC (norms n[m]): the scales that bring phi to the next
+// step, phi_m <- sc_m phi_m.
+//  real time: 1.
+//  imaginary time with SOC: NORMT, sc_m = 1/sqrt(sum n) (cgpe1d.f90:472).
+//  imaginary time without SOC: projection PHI_m <- SIGMA_m PHI_m, then NORMT
+//  (cgpe1d.f90:443-470): spin-1 closed form (cgpe1d.f90:447-450; the 3D
+//  program places EPS inside the square root, cgpe3d.f90:464-465), spin-2
+//  SIGMA_m = exp((SIG1 + c_m SIG2) DT) with SIG from the Newton-Raphson solve
+//  of NEWTON/USRFUN (cgpe1d.f90:1245-1319), started from the previous step's
+//  SIG (20, 20 initially), NTRIAL = 1000, TOL_NR = 1e-6.
+// Returns 0, or 2 when the Newton iteration did not converge.
+template <int MS>
+__device__ int compute_scales(const StepConst& c, const double* n, double* sig, double* sc) {
+    double tot = 0;
+    for (int m = 0; m < MS; ++m) tot += n[m];
+    if (!c.imag) { for (int m = 0; m < MS; ++m) sc[m] = 1.0; return 0; }
+    if (!c.project) { const double s = 1.0 / sqrt(tot); for (int m = 0; m < MS; ++m) sc[m] = s; return 0; }
+    const double EPSV = 1.0e-40, mag = c.mag;
+    double sg[MS];
+    int rc = 0;
+    if constexpr (MS == 3) {
+        const double inner = sqrt(4.0 * (1.0 - mag * mag) * n[0] * n[2] + mag * mag * n[1] * n[1]);
+        if (c.dim == 3) sg[1] = sqrt(1.0 - mag * mag) / sqrt(n[1] + inner + EPSV);
+        else sg[1] = sqrt(1.0 - mag * mag) / (sqrt(n[1] + inner) + EPSV);
+        sg[0] = sqrt(1.0 + mag - sg[1] * sg[1] * n[1]) / (sqrt(2.0 * n[0]) + EPSV);
+        sg[2] = sqrt(1.0 - mag - sg[1] * sg[1] * n[1]) / (sqrt(2.0 * n[2]) + EPSV);
+    } else {
+        const double dt = c.dt;
+        double x1 = sig[0], x2 = sig[1], p1 = 0, p2 = 0;
+        for (int k = 0; k < 1000; ++k) {
+            const double e1 = exp(2.0 * (x1 + 2.0 * x2) * dt), e2 = exp(2.0 * (x1 + x2) * dt), e3 = exp(2.0 * x1 * dt),
+                         e4 = exp(2.0 * (x1 - x2) * dt), e5 = exp(2.0 * (x1 - 2.0 * x2) * dt);
+            const double f1 = e1 * n[0] + e2 * n[1] + e3 * n[2] + e4 * n[3] + e5 * n[4] - 1.0;
+            const double f2 = 2.0 * e1 * n[0] + e2 * n[1] - e4 * n[3] - 2.0 * e5 * n[4] - mag;
+            const double j11 = (e1 * n[0] + e2 * n[1] + e3 * n[2] + e4 * n[3] + e5 * n[4]) * 2.0 * dt;
+            const double j12 = e1 * n[0] * 4.0 * dt + e2 * n[1] * 2.0 * dt + e4 * n[3] * (-2.0 * dt) + e5 * n[4] * (-4.0 * dt);
+            const double j21 = (2.0 * e1 * n[0] + e2 * n[1] - e4 * n[3] - 2.0 * e5 * n[4]) * 2.0 * dt;
+            const double j22 = 2.0 * e1 * n[0] * 4.0 * dt + e2 * n[1] * 2.0 * dt - e4 * n[3] * (-2.0 * dt)
+                               - 2.0 * e5 * n[4] * (-4.0 * dt);
+            p2 = (f2 * j11 - f1 * j21) / (j21 * j12 - j11 * j22);
+            p1 = (-f1 - j12 * p2) / j11;
+            x1 += p1; x2 += p2;
+            if (fmax(fabs(p1), fabs(p2)) <= 1.0e-6) break;
+        }
+        if (fmax(fabs(p1), fabs(p2)) > 1.0e-6) rc = 2;
+        sig[0] = x1; sig[1] = x2;
+        for (int m = 0; m < MS; ++m) sg[m] = exp((x1 + (2 - m) * x2) * dt);
+    }
+    double t2 = 0;
+    for (int m = 0; m < MS; ++m) t2 += sg[m] * sg[m] * n[m];
+    const double inv = 1.0 / sqrt(t2);
+    for (int m = 0; m < MS; ++m) sc[m] = sg[m] * inv;
+    return rc;
 }
 
 }  // namespace fgpe

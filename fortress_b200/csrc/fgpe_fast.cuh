@@ -148,7 +148,7 @@ template <int N> __device__ __forceinline__ void cp_wait() { asm volatile("cp.as
 #define FGPE_COL_NBUF 1
 #endif
 #ifndef FGPE_TW_SMEM
-#define FGPE_TW_SMEM 1
+#define FGPE_TW_SMEM 0
 #endif
 
 // ------------------------------------------------------------ row kernel
@@ -290,8 +290,9 @@ __global__ void __launch_bounds__(TH, FGPE_COL_MINB) k_col_fast(StepConst c, Col
         tw = tws;
     }
     cx<T>* S = (cx<T>*)a.S;
-    T fac = (T)1;
-    if (a.flags & COL_SCALE) fac = (T)(a.info[INFO_SCALE] * a.cfac);
+    T fac[MS];
+#pragma unroll
+    for (int m = 0; m < MS; ++m) fac[m] = (a.flags & COL_SCALE) ? (T)(a.info[INFO_SC + m] * a.cfac) : (T)1;
 
     auto issue = [&](int tile, cx<T>* dst) {
         const int x0 = (tile % nxt) * TX;
@@ -329,7 +330,7 @@ __global__ void __launch_bounds__(TH, FGPE_COL_MINB) k_col_fast(StepConst c, Col
             for (int idx = threadIdx.x; idx < MS * N * TX; idx += TH) {
                 const int t = idx % TX, q = idx / TX, e = q % N, m = q / N;
                 cx<T>& v = cur[(m * LPN + e + (e >> 3)) * TX + t];
-                v = cscale(v, fac);
+                v = cscale(v, fac[m]);
             }
             __syncthreads();
         }

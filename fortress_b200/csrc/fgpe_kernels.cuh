@@ -70,12 +70,14 @@ __device__ __forceinline__ void finish_norms(const StepConst& c, const double* p
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        double tot = 0;
-        for (int m = 0; m < MS; ++m) { tot += red[m]; info[INFO_NORM + m] = red[m]; }
+        double tot = 0, n[MS], sc[MS];
+        for (int m = 0; m < MS; ++m) { n[m] = red[m]; tot += red[m]; info[INFO_NORM + m] = red[m]; }
         info[INFO_TOTAL] = tot;
-        double sc = c.imag ? 1.0 / sqrt(tot) : 1.0;
-        if (!(tot == tot) || !(tot < 1e300) || !(sc == sc)) info[INFO_ERR] = 1.0;
-        info[INFO_SCALE] = sc;
+        const int rc = compute_scales<MS>(c, n, info + INFO_SIG, sc);
+        bool bad = !(tot == tot) || !(tot < 1e300);
+        for (int m = 0; m < MS; ++m) { info[INFO_SC + m] = sc[m]; bad = bad || !(sc[m] == sc[m]); }
+        if (bad) info[INFO_ERR] = 1.0;
+        if (rc) info[INFO_ERR] = (double)rc;
         *counter = 0u;
     }
 }
@@ -178,12 +180,13 @@ k_col(StepConst c, ColArgs a) {
     const cx<T>* tw = (const cx<T>*)a.tw;
     const int nel = MS * n * TX;
     cx<T>* S = (cx<T>*)a.S;
-    T fac = (T)1;
-    if (a.flags & COL_SCALE) fac = (T)(a.info[INFO_SCALE] * a.cfac);
+    T fac[MS];
+#pragma unroll
+    for (int m = 0; m < MS; ++m) fac[m] = (a.flags & COL_SCALE) ? (T)(a.info[INFO_SC + m] * a.cfac) : (T)1;
     for (int idx = threadIdx.x; idx < nel; idx += blockDim.x) {
         const int t = idx % TX, q = idx / TX, e = q % n, m = q / n;
         cx<T> v = S[(size_t)m * np + off + (size_t)e * a.axis_stride + t];
-        if (a.flags & COL_SCALE) v = cscale(v, fac);
+        if (a.flags & COL_SCALE) v = cscale(v, fac[m]);
         sm[(m * lpn + pad_idx(e)) * TX + t] = v;
     }
     __syncthreads();
@@ -223,16 +226,15 @@ k_1d(StepConst c, OneDArgs a) {
     cx<T>* sm = (cx<T>*)smraw;
     __shared__ double red[32 * (MS + 1)];
     __shared__ double bsum[MS];
-    __shared__ double s_scale;
+    __shared__ double s_sc[MS];
     const int nx = c.nx;
     const int lp = padded_len(nx);
     const RowMap mp{lp};
     const cx<T>* tw = (const cx<T>*)c.twx;
     cx<T>* psi = (cx<T>*)a.psi;
-    const T sc0 = (T)a.info[INFO_SCALE];
     for (int idx = threadIdx.x; idx < MS * nx; idx += blockDim.x) {
         const int x = idx % nx, m = idx / nx;
-        sm[m * lp + pad_idx(x)] = cscale(psi[(size_t)m * nx + x], sc0);
+        sm[m * lp + pad_idx(x)] = cscale(psi[(size_t)m * nx + x], (T)a.info[INFO_SC + m]);
     }
     __syncthreads();
     const T invn = (T)(1.0 / nx);
@@ -268,9 +270,11 @@ k_1d(StepConst c, OneDArgs a) {
         }
         block_sum<MS>(acc, red, bsum);
         if (threadIdx.x == 0) {
-            double tot = 0;
-            for (int m = 0; m < MS; ++m) tot += bsum[m];
-            s_scale = c.imag ? 1.0 / sqrt(tot) : 1.0;
+            double tot = 0, n[MS], sc[MS];
+            for (int m = 0; m < MS; ++m) { n[m] = bsum[m]; tot += bsum[m]; }
+            const int rc = compute_scales<MS>(c, n, a.info + INFO_SIG, sc);
+            for (int m = 0; m < MS; ++m) s_sc[m] = sc[m];
+            if (rc) a.info[INFO_ERR] = (double)rc;
             if (step == a.nsteps - 1) {
                 for (int m = 0; m < MS; ++m) a.info[INFO_NORM + m] = bsum[m];
                 a.info[INFO_TOTAL] = tot;
@@ -279,15 +283,14 @@ k_1d(StepConst c, OneDArgs a) {
         }
         __syncthreads();
         if (c.imag) {
-            const T s = (T)s_scale;
             for (int idx = threadIdx.x; idx < MS * nx; idx += blockDim.x) {
                 const int x = idx % nx, m = idx / nx;
-                sm[m * lp + pad_idx(x)] = cscale(sm[m * lp + pad_idx(x)], s);
+                sm[m * lp + pad_idx(x)] = cscale(sm[m * lp + pad_idx(x)], (T)s_sc[m]);
             }
             __syncthreads();
         }
         if (a.snap_prev && step == a.nsteps - 2) {
-            if (threadIdx.x == 0) a.info_prev[INFO_SCALE] = 1.0;
+            if (threadIdx.x < MS) a.info_prev[INFO_SC + threadIdx.x] = 1.0;
             cx<T>* sp = (cx<T>*)a.snap_prev;
             for (int idx = threadIdx.x; idx < MS * nx; idx += blockDim.x) {
                 const int x = idx % nx, m = idx / nx;
@@ -299,7 +302,7 @@ k_1d(StepConst c, OneDArgs a) {
         const int x = idx % nx, m = idx / nx;
         psi[(size_t)m * nx + x] = sm[m * lp + pad_idx(x)];
     }
-    if (threadIdx.x == 0) a.info[INFO_SCALE] = 1.0;
+    if (threadIdx.x < MS) a.info[INFO_SC + threadIdx.x] = 1.0;
 }
 
 // ------------------------------------------------------------ observables
@@ -368,8 +371,9 @@ k_obs(StepConst c, ObsArgs a) {
     const long long np = c.npts;
     const cx<T>* psi = (const cx<T>*)a.psi;
     const cx<T>* prev = (const cx<T>*)a.prev;
-    const double s = a.info[INFO_SCALE];
-    const double sp = prev ? a.info_prev[INFO_SCALE] : 0.0;
+    double s_m[MS], sp_m[MS];
+#pragma unroll
+    for (int m = 0; m < MS; ++m) { s_m[m] = a.info[INFO_SC + m]; sp_m[m] = prev ? a.info_prev[INFO_SC + m] : 0.0; }
     double acc[NQ];
 #pragma unroll
     for (int q = 0; q < NQ; ++q) acc[q] = 0.0;
@@ -383,10 +387,10 @@ k_obs(StepConst c, ObsArgs a) {
 #pragma unroll
         for (int m = 0; m < MS; ++m) {
             const cx<T> v = psi[(size_t)m * np + t];
-            P[m] = make_double2(s * (double)v.x, s * (double)v.y);
+            P[m] = make_double2(s_m[m] * (double)v.x, s_m[m] * (double)v.y);
             if (prev) {
                 const cx<T> u = prev[(size_t)m * np + t];
-                const double dx = P[m].x - sp * (double)u.x, dy = P[m].y - sp * (double)u.y;
+                const double dx = P[m].x - sp_m[m] * (double)u.x, dy = P[m].y - sp_m[m] * (double)u.y;
                 cmax = fmax(cmax, sqrt(dx * dx + dy * dy));
             }
         }
@@ -406,6 +410,7 @@ k_obs(StepConst c, ObsArgs a) {
 #pragma unroll
             for (int m = 0; m < MS; ++m) {
                 const cx<T>* pm = psi + (size_t)m * np;
+                const double s = s_m[m];
                 auto lx = [&](int q) { cx<T> v = pm[base + q]; return make_double2(s * (double)v.x, s * (double)v.y); };
                 X[m] = dline<T>(lx, i, c.nx, a.dx);
                 Y[m] = make_double2(0, 0); Z[m] = make_double2(0, 0);
@@ -521,23 +526,20 @@ k_obs(StepConst c, ObsArgs a) {
         o[OBS_CONV] = red[NQ];
         o[OBS_TOTAL] = tot;
         if (a.mode == OBS_NORMALIZE) {
-            // NORMT: the pending scale absorbs 1/sqrt(total)
-            a.info[INFO_SCALE] = a.info[INFO_SCALE] / sqrt(tot);
+            // NORMT: the pending scales absorb 1/sqrt(total)
+            for (int m = 0; m < MS; ++m) a.info[INFO_SC + m] = a.info[INFO_SC + m] / sqrt(tot);
         }
         *a.counter = 0u;
     }
 }
 
-// scale psi by info[INFO_SCALE] (used after NORMT in 1D, where the state is
-// kept normalised explicitly) and reset the scale to 1.
+// psi_m <- sc_m psi_m (folds the pending scales into the state); n2 counts
+// reals, per2 = 2*NPTS reals per component.
 template <typename T>
-__global__ void k_apply_scale(T* psi, long long n2, double* info) {
-    const double s = info[INFO_SCALE];
+__global__ void k_apply_scale(T* psi, long long n2, long long per2, double* info) {
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n2; t += (long long)gridDim.x * blockDim.x)
-        psi[t] = (T)(s * (double)psi[t]);
+        psi[t] = (T)(info[INFO_SC + t / per2] * (double)psi[t]);
 }
-template <typename T>
-__global__ void k_reset_scale(double* info) { info[INFO_SCALE] = 1.0; }
 
 // Unfused single operators on a full real/Fourier-space buffer (parity
 // checks of individual reference subroutines).

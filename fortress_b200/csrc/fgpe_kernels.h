@@ -6,10 +6,11 @@ namespace fgpe {
 
 // Layout of the per-handle device "info" vector (doubles).
 enum {
-    INFO_SCALE = 0,   // pending renormalisation: phi = scale * psi
     INFO_TOTAL = 1,   // sum of the norms of the last step (before NORMT)
-    INFO_ERR = 2,     // non-finite reduction seen
-    INFO_NORM = 3,    // NORMC of the last step, MS values
+    INFO_ERR = 2,     // 1: non-finite reduction, 2: Newton projection failed
+    INFO_NORM = 3,    // NORMC of the last step, MS values (3..7)
+    INFO_SC = 8,      // pending per-component scale: phi_m = sc_m * psi_m (8..12)
+    INFO_SIG = 13,    // SIG(1:2) of the spin-2 magnetisation projection (13, 14)
     INFO_LEN = 16
 };
 

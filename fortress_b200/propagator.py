@@ -33,7 +33,7 @@ def _dp(a):
 
 class Propagator:
     def __init__(self, dim, spin, n, d, dt, imag_time, tau, gamma=(0.0, 0.0, 0.0),
-                 alpha=(1.0, 1.0, 1.0), precision="fp64", kernels="auto"):
+                 alpha=(1.0, 1.0, 1.0), precision="fp64", kernels="auto", mag=0.0):
         L = _abi.load()
         p = _abi.Params()
         n = list(n) + [1] * (3 - len(n))
@@ -51,6 +51,7 @@ class Propagator:
             p.alpha[i] = float(alpha[i])
         p.precision = _abi.FGPE_FP32 if str(precision).lower() in ("fp32", "float32", "1") else _abi.FGPE_FP64
         p.kernels = {"auto": 0, "generic": 1, "fast-row": 2, "fast-col": 3}[kernels]
+        p.mag = float(mag)
         self.params = p
         self.dim, self.spin, self.ms = p.dim, p.spin, 2 * p.spin + 1
         self.shape = (p.nx, p.ny if p.dim >= 2 else 1, p.nz if p.dim >= 3 else 1)

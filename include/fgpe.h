@@ -35,7 +35,9 @@ enum {
     FGPE_E_ARG = -1,        /* invalid argument / unsupported size */
     FGPE_E_CUDA = -2,       /* CUDA runtime error (message in fgpe_last_error) */
     FGPE_E_STATE = -3,      /* call out of order (e.g. no state set) */
-    FGPE_E_NONFINITE = -4   /* a reduction produced NaN/Inf */
+    FGPE_E_NONFINITE = -4,  /* a reduction produced NaN/Inf */
+    FGPE_E_NEWTON = -5      /* spin-2 magnetisation projection: Newton-Raphson
+                               did not converge (cgpe1d.f90:1287-1290) */
 };
 
 enum { FGPE_FP64 = 0, FGPE_FP32 = 1 };
@@ -67,7 +69,9 @@ typedef struct fgpe_params {
     int kernels;        /* FGPE_KERNELS_AUTO: size-specialised persistent
                            kernels where compiled, else generic;
                            FGPE_KERNELS_GENERIC: generic kernels only */
-    int reserved[6];
+    double mag;         /* MAG: magnetisation imposed in imaginary time when
+                           all GAMMA are zero (cgpe1d.f90:257, 443-470) */
+    int reserved[4];
 } fgpe_params;
 
 typedef struct fgpe_s fgpe_t;

@@ -130,6 +130,9 @@ typedef struct {
     double *x, *y, *z, *kx, *ky, *kz;
     cd *phi;                   /* PHI(NX,NY,NZ,MS) */
     fftplan px, py, pz;
+    int switch_soc;            /* cgpe1d.f90:250 */
+    double mag;                /* MAG */
+    double sig[2];             /* SIG(1:2), cgpe1d.f90:425-426 */
 } orc_t;
 
 static inline long IDX(const orc_t *h, int i, int j, int k) {
@@ -161,6 +164,10 @@ orc_t *orc_create(const orc_params *p) {
     if (h->p.dim >= 3) { make_k(h->kz, h->p.nz, h->p.nz * h->p.dz); make_x(h->z, h->p.nz, h->p.nz * h->p.dz); }
     h->phi = (cd *)calloc((size_t)h->npts * h->ms, sizeof(cd));
     plan_init(&h->px, h->p.nx); plan_init(&h->py, h->p.ny); plan_init(&h->pz, h->p.nz);
+    /* cgpe1d.f90:250, cgpe2d.f90:251, cgpe3d.f90:256 */
+    h->switch_soc = fabs(p->gx) > EPS || (p->dim >= 2 && fabs(p->gy) > EPS) || (p->dim >= 3 && fabs(p->gz) > EPS);
+    h->mag = 0.0;
+    h->sig[0] = h->sig[1] = 20.0;
     return h;
 }
 
@@ -817,15 +824,75 @@ void orc_energy(const orc_t *h, double *mu, double *en, double *mz) {
     free(f); free(gx); free(gy); free(gz);
 }
 
+void orc_set_mag(orc_t *h, double mag) { h->mag = mag; }
+void orc_get_sig(const orc_t *h, double *sig) { sig[0] = h->sig[0]; sig[1] = h->sig[1]; }
+
+/* USRFUN, cgpe1d.f90:1292-1319 */
+static void usrfun(const double *x, double *fvec, double fjac[2][2], const double *n, double mag, double dt) {
+    double e1 = exp(2.0 * (x[0] + 2.0 * x[1]) * dt), e2 = exp(2.0 * (x[0] + x[1]) * dt), e3 = exp(2.0 * x[0] * dt);
+    double e4 = exp(2.0 * (x[0] - x[1]) * dt), e5 = exp(2.0 * (x[0] - 2.0 * x[1]) * dt);
+    fvec[0] = e1 * n[0] + e2 * n[1] + e3 * n[2] + e4 * n[3] + e5 * n[4] - 1.0;
+    fvec[1] = 2.0 * e1 * n[0] + e2 * n[1] - e4 * n[3] - 2.0 * e5 * n[4] - mag;
+    fjac[0][0] = (e1 * n[0] + e2 * n[1] + e3 * n[2] + e4 * n[3] + e5 * n[4]) * 2.0 * dt;
+    fjac[0][1] = e1 * n[0] * 4.0 * dt + e2 * n[1] * 2.0 * dt + e4 * n[3] * (-2.0 * dt) + e5 * n[4] * (-4.0 * dt);
+    fjac[1][0] = (2.0 * e1 * n[0] + e2 * n[1] - e4 * n[3] - 2.0 * e5 * n[4]) * 2.0 * dt;
+    fjac[1][1] = 2.0 * e1 * n[0] * 4.0 * dt + e2 * n[1] * 2.0 * dt - e4 * n[3] * (-2.0 * dt) - 2.0 * e5 * n[4] * (-4.0 * dt);
+}
+
+/* NEWTON, cgpe1d.f90:1245-1291 (NTRIAL = 1000, TOL_NR = 1e-6).  Returns 1
+ * when the root was not found within tolerance (ERR_MSG). */
+static int newton(double *x, const double *n, double mag, double dt) {
+    double p[2] = {0, 0}, fvec[2], fjac[2][2];
+    for (int k = 0; k < 1000; ++k) {
+        usrfun(x, fvec, fjac, n, mag, dt);
+        p[1] = (fvec[1] * fjac[0][0] - fvec[0] * fjac[1][0]) / (fjac[1][0] * fjac[0][1] - fjac[0][0] * fjac[1][1]);
+        p[0] = (-fvec[0] - fjac[0][1] * p[1]) / fjac[0][0];
+        x[0] += p[0]; x[1] += p[1];
+        if (fmax(fabs(p[0]), fabs(p[1])) <= 1.0e-6) break;
+    }
+    return fmax(fabs(p[0]), fabs(p[1])) > 1.0e-6;
+}
+
+/* Projection of the imaginary-time no-SOC branch, cgpe1d.f90:444-469
+ * (3D spin-1 EPS placement cgpe3d.f90:464-465). */
+static int project(orc_t *h, const double *norm) {
+    double sg[5];
+    const double mag = h->mag;
+    if (h->p.spin == 1) {
+        double inner = sqrt(4.0 * (1.0 - mag * mag) * norm[0] * norm[2] + mag * mag * norm[1] * norm[1]);
+        if (h->p.dim == 3) sg[1] = sqrt(1.0 - mag * mag) / sqrt(norm[1] + inner + EPS);
+        else sg[1] = sqrt(1.0 - mag * mag) / (sqrt(norm[1] + inner) + EPS);
+        sg[0] = sqrt(1.0 + mag - sg[1] * sg[1] * norm[1]) / (sqrt(2.0 * norm[0]) + EPS);
+        sg[2] = sqrt(1.0 - mag - sg[1] * sg[1] * norm[1]) / (sqrt(2.0 * norm[2]) + EPS);
+    } else {
+        if (newton(h->sig, norm, mag, h->p.dt)) return 1;
+        sg[0] = exp((h->sig[0] + 2.0 * h->sig[1]) * h->p.dt);
+        sg[1] = exp((h->sig[0] + h->sig[1]) * h->p.dt);
+        sg[2] = exp(h->sig[0] * h->p.dt);
+        sg[3] = exp((h->sig[0] - h->sig[1]) * h->p.dt);
+        sg[4] = exp((h->sig[0] - 2.0 * h->sig[1]) * h->p.dt);
+    }
+    const long np = h->npts;
+    for (int m = 0; m < h->ms; ++m)
+        for (long t = 0; t < np; ++t) h->phi[t + m * np] *= sg[m];
+    return 0;
+}
+
 /* ----------------------------------------------------- one split step */
 /* cgpe1d.f90:434-441 then 443-474 (imaginary time with SOC: NORMT only).
  * norm_out receives NORMC before the renormalisation (what file3 reports). */
-void orc_step(orc_t *h, int nsteps, double *norm_out) {
+int orc_step(orc_t *h, int nsteps, double *norm_out) {
+    double nbuf[5];
     for (int s = 0; s < nsteps; ++s) {
         orc_fft(h); orc_ke(h); orc_soc(h); orc_bft(h); orc_se(h); orc_sp(h);
-        if (norm_out) orc_normc(h, norm_out);
-        if (h->p.imag) orc_normt(h);
+        double *n = norm_out ? norm_out : nbuf;
+        orc_normc(h, n);
+        if (h->p.imag) {
+            if (!h->switch_soc && project(h, n)) return 1;   /* ERR_MSG -> STOP */
+            orc_normt(h);
+        }
     }
+    return 0;
 }
 
 /* max |phi - other| over all points and components (CONV numerator,

@@ -59,6 +59,9 @@ def lib():
         L.orc_rad.argtypes = [ctypes.c_void_p, P]
         L.orc_energy.argtypes = [ctypes.c_void_p, P, P, P]
         L.orc_step.argtypes = [ctypes.c_void_p, ctypes.c_int, P]
+        L.orc_step.restype = ctypes.c_int
+        L.orc_set_mag.argtypes = [ctypes.c_void_p, ctypes.c_double]
+        L.orc_get_sig.argtypes = [ctypes.c_void_p, P]
         L.orc_maxdiff.restype = ctypes.c_double
         L.orc_maxdiff.argtypes = [ctypes.c_void_p, P]
         L.orc_initialize.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double]
@@ -241,8 +244,15 @@ class Oracle:
 
     def step(self, n=1):
         norm = np.zeros(self.ms)
-        lib().orc_step(self.h, int(n), _dp(norm))
+        if lib().orc_step(self.h, int(n), _dp(norm)):
+            raise RuntimeError("Newton-Raphson projection did not converge")
         return norm
+
+    def set_mag(self, mag):
+        lib().orc_set_mag(self.h, float(mag))
+
+    def sig(self):
+        s = np.zeros(2); lib().orc_get_sig(self.h, _dp(s)); return s
 
     def maxdiff(self, other):
         flat = np.ascontiguousarray(np.asarray(other, np.complex128).reshape(-1, order="F"))

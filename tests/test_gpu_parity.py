@@ -131,3 +131,32 @@ def test_fast_matches_generic_512(F, precision):
     a.step(20); b.step(20)
     tol = 1e-12 if precision == "fp64" else 1e-5
     assert rel_err(a.state(), b.state()) < tol
+
+
+PROJ_CASES = [(1, 1, 1, (96,)), (1, 2, 1, (64,)), (2, 1, 1, (32, 24)), (2, 2, 1, (32, 32)),
+              (3, 1, 1, (16, 16, 12)), (3, 2, 1, (16, 12, 16)), (2, 2, 1, (128, 192))]
+
+
+@pytest.mark.parametrize("case", PROJ_CASES, ids=case_id)
+def test_projection_branch(F, case):
+    """Imaginary time without SOC: SIGMA projection to the imposed MAG
+    (spin-1 closed form, spin-2 Newton) before NORMT, cgpe1d.f90:443-470."""
+    p = case_params(case)
+    p["gamma"] = (0.0,) * case[0]
+    mag = 0.3 if case[1] == 2 else 0.2
+    orc = O.Oracle(**oracle_kwargs(p))
+    phi = initial_state(orc, 1)
+    orc.set_state(phi)
+    orc.set_mag(mag)
+    prop = F.Propagator(**p, mag=mag)
+    prop.set_state(phi)
+    orc.normt(); prop.normt()
+    for batch in (1, 6):
+        norm_o = orc.step(batch)
+        prop.step(batch)
+        assert np.allclose(prop.normc(), norm_o, rtol=1e-11, atol=0)
+        assert rel_err(prop.state(), orc.state()) < 1e-11
+    en_g, mu_g, mz_g, _ = prop.observables()
+    en_o, mu_o, mz_o = orc.energy()
+    assert abs(mz_g - mag) < 1e-12 and abs(mz_o - mag) < 1e-12
+    assert abs(en_g - en_o) <= 1e-10 * abs(en_o)
