@@ -35,6 +35,9 @@ EXPORTS = (
     "fgpe_step", "fgpe_step_ex", "fgpe_normalize", "fgpe_norms", "fgpe_observables",
     "fgpe_conv", "fgpe_center", "fgpe_apply_op", "fgpe_version", "fgpe_device_ok",
     "fgpe_kernel_launches", "fgpe_norms_async", "fgpe_profile_enable", "fgpe_profile_read",
+    "fgpe_batch_create", "fgpe_batch_destroy", "fgpe_batch_size", "fgpe_batch_instance",
+    "fgpe_batch_last_error", "fgpe_batch_config", "fgpe_batch_step", "fgpe_batch_observables",
+    "fgpe_batch_autotune", "fgpe_batch_tuning", "fgpe_set_kernels",
 )
 
 
@@ -89,6 +92,17 @@ def load():
         "fgpe_norms_async": ([vp, vp], ip),
         "fgpe_profile_enable": ([vp, ip], ip),
         "fgpe_profile_read": ([vp, dp, ctypes.POINTER(ctypes.c_longlong), ip], ip),
+        "fgpe_batch_create": ([ctypes.POINTER(Params), ip, ctypes.POINTER(vp)], ip),
+        "fgpe_batch_destroy": ([vp], ip),
+        "fgpe_batch_size": ([vp], ip),
+        "fgpe_batch_instance": ([vp, ip, ctypes.POINTER(vp)], ip),
+        "fgpe_batch_last_error": ([vp], ctypes.c_char_p),
+        "fgpe_batch_config": ([vp, ip, ip], ip),
+        "fgpe_batch_step": ([vp, ip], ip),
+        "fgpe_batch_observables": ([vp, dp, ip], ip),
+        "fgpe_batch_autotune": ([vp, ip, ctypes.c_char_p], ip),
+        "fgpe_batch_tuning": ([vp, ctypes.POINTER(ip), ctypes.POINTER(ip)], ip),
+        "fgpe_set_kernels": ([vp, ip], ip),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -101,5 +115,12 @@ def load():
 def check(rc, handle=None):
     if rc != FGPE_OK:
         msg = load().fgpe_last_error(handle)
+        raise FgpeError(rc, msg.decode() if msg else "")
+    return rc
+
+
+def check_batch(rc, batch=None):
+    if rc != FGPE_OK:
+        msg = load().fgpe_batch_last_error(batch)
         raise FgpeError(rc, msg.decode() if msg else "")
     return rc

@@ -1,0 +1,83 @@
+"""Batched sweeps: many independent instances advanced by one CUDA-graph
+launch per group of steps (C ABI: fgpe_batch_* in include/fgpe.h).
+
+The reference runs one parameter point per process; a phase-diagram sweep
+over spin-orbit strengths, couplings and trap anisotropies with uneven grid
+sizes is a batch here.  Each instance is a full :class:`Propagator`.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _abi
+from ._abi import check_batch
+from .propagator import Propagator, make_params
+
+
+class Batch:
+    def __init__(self, instances):
+        """instances: list of keyword dicts for :class:`Propagator`."""
+        L = _abi.load()
+        arr = (_abi.Params * len(instances))()
+        for i, kw in enumerate(instances):
+            arr[i] = make_params(**kw)
+        b = ctypes.c_void_p()
+        check_batch(L.fgpe_batch_create(arr, len(instances), ctypes.byref(b)))
+        self._b, self._L = b, L
+        self.props = []
+        for i, kw in enumerate(instances):
+            h = ctypes.c_void_p()
+            check_batch(L.fgpe_batch_instance(b, i, ctypes.byref(h)), b)
+            self.props.append(Propagator(**kw, _handle=h, _owner=self))
+
+    def __len__(self):
+        return len(self.props)
+
+    def __getitem__(self, i):
+        return self.props[i]
+
+    def close(self):
+        if getattr(self, "_b", None):
+            for p in self.props:
+                p._h = None
+            self._L.fgpe_batch_destroy(self._b)
+            self._b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def config(self, width=0, steps_per_graph=0):
+        check_batch(self._L.fgpe_batch_config(self._b, int(width), int(steps_per_graph)), self._b)
+
+    def tuning(self):
+        w, k = ctypes.c_int(), ctypes.c_int()
+        check_batch(self._L.fgpe_batch_tuning(self._b, ctypes.byref(w), ctypes.byref(k)), self._b)
+        return w.value, k.value
+
+    def autotune(self, trial_steps=8, cache_path=None):
+        c = cache_path.encode() if cache_path else None
+        check_batch(self._L.fgpe_batch_autotune(self._b, int(trial_steps), c), self._b)
+        return self.tuning()
+
+    def step(self, n):
+        check_batch(self._L.fgpe_batch_step(self._b, int(n)), self._b)
+
+    def observables(self, with_conv=True):
+        """Per instance: dict(en, mz, conv, mu, rms, norm)."""
+        ms = [p.ms for p in self.props]
+        stride = [3 + 3 * m for m in ms]
+        out = np.zeros(sum(stride))
+        check_batch(self._L.fgpe_batch_observables(self._b, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                                   int(bool(with_conv))), self._b)
+        res, o = [], 0
+        for m, s in zip(ms, stride):
+            v = out[o:o + s]
+            res.append(dict(en=v[0], mz=v[1], conv=v[2], mu=v[3:3 + m].copy(), rms=v[3 + m:3 + 2 * m].copy(),
+                            norm=v[3 + 2 * m:3 + 3 * m].copy()))
+            o += s
+        return res

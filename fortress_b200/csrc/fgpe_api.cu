@@ -54,6 +54,7 @@ struct fgpe_s {
     double* h_small = nullptr;   // pinned, 64 doubles
     Launch row, col[3], k1, obsl;
     bool fast_row = false, fast_col[3] = {false, false, false};
+    bool has_fast_row = false, has_fast_col[3] = {false, false, false};
     int fast_row_grid = 0, fast_col_grid[3] = {0, 0, 0};
     bool psi_valid = false, S_valid = false, prev_valid = false, norms_valid = false, has_state = false;
     long long launches = 0;
@@ -609,7 +610,7 @@ int fgpe_create(const fgpe_params* pin, fgpe_t** out) {
                              : (ms == 3 ? setup_fast_row<double, 3, NN>(h) : setup_fast_row<double, 5, NN>(h))
         FAST_SWITCH(p.nx, SETR)
 #undef SETR
-        if (g > 0) { h->fast_row = true; h->fast_row_grid = g; }
+        if (g > 0) { h->fast_row = h->has_fast_row = true; h->fast_row_grid = g; }
     }
     for (int a = 1; a < p.dim; ++a) {
         if (!allow_fast_col || !fast_size(ns[a])) continue;
@@ -619,7 +620,7 @@ int fgpe_create(const fgpe_params* pin, fgpe_t** out) {
                              : (ms == 3 ? setup_fast_col<double, 3, NN>(h, ntl) : setup_fast_col<double, 5, NN>(h, ntl))
         FAST_SWITCH(ns[a], SETC)
 #undef SETC
-        if (g > 0) { h->fast_col[a] = true; h->fast_col_grid[a] = g; }
+        if (g > 0) { h->fast_col[a] = h->has_fast_col[a] = true; h->fast_col_grid[a] = g; }
     }
     cudaGetLastError();   // clear any attribute/occupancy probe error
     h->obsl.grid = dim3((unsigned)((h->npts + 255) / 256));
@@ -774,7 +775,10 @@ int fgpe_step_ex(fgpe_t* h, int nsteps, int flags) {
         h->S_valid = true;
     }
     h->prev_valid = false;
-    if (snap && h->psi_valid) {
+    // one step: the state before the call becomes the CONV reference; with
+    // two or more steps the row pass of step n-1 writes it anyway (and the
+    // buffers keep their roles, which CUDA-graph replays rely on)
+    if (snap && h->psi_valid && nsteps == 1) {
         std::swap(h->psi, h->prev);
         CK(cudaMemcpyAsync(h->info_prev, h->info, INFO_LEN * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
         h->prev_valid = true;
@@ -930,6 +934,14 @@ int fgpe_apply_op(fgpe_t* h, int op) {
     return FGPE_OK;
 }
 
+int fgpe_set_kernels(fgpe_t* h, int kernels) {
+    if (!h) return fail(h, FGPE_E_ARG, "null handle");
+    const bool fast = kernels != FGPE_KERNELS_GENERIC;
+    h->fast_row = fast && h->has_fast_row && kernels != FGPE_KERNELS_FAST_COL_ONLY;
+    for (int a = 0; a < 3; ++a) h->fast_col[a] = fast && h->has_fast_col[a] && kernels != FGPE_KERNELS_FAST_ROW_ONLY;
+    return FGPE_OK;
+}
+
 int fgpe_norms_async(fgpe_t* h, double* dst) {
     if (!h || !dst) return fail(h, FGPE_E_ARG, "null argument");
     if (!h->norms_valid) return fail(h, FGPE_E_STATE, "no step taken since the state was set");
@@ -970,6 +982,331 @@ int fgpe_debug_align_fault(unsigned long long* out4) {
     return FGPE_OK;
 }
 #endif
+
+// ================================================================ batches
+}  // extern "C"
+
+struct fgpe_batch_s {
+    std::vector<fgpe_t*> inst;
+    cudaStream_t origin = nullptr;
+    std::vector<cudaStream_t> lanes;
+    std::vector<cudaEvent_t> ev;            // fork/join events, one per lane + 1
+    int width = 0;                          // concurrent branches
+    int ksteps = 0;                         // steps per captured graph
+    cudaGraphExec_t exec = nullptr;
+    int exec_steps = 0;
+    std::string msg;
+};
+
+namespace {
+int bfail(fgpe_batch_t* b, int code, const std::string& m) {
+    if (b) b->msg = m;
+    g_last_error = m;
+    return code;
+}
+#define BCK(call)                                                                              \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess) return bfail(b, FGPE_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+void drop_graph(fgpe_batch_t* b) {
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    b->exec = nullptr;
+    b->exec_steps = 0;
+}
+
+int set_width(fgpe_batch_t* b, int w) {
+    w = std::max(1, std::min<int>(w, (int)b->inst.size()));
+    if (w == b->width) return FGPE_OK;
+    drop_graph(b);
+    for (cudaStream_t s : b->lanes) cudaStreamDestroy(s);
+    for (cudaEvent_t e : b->ev) cudaEventDestroy(e);
+    b->lanes.assign(w, nullptr);
+    b->ev.assign(2 * w + 1, nullptr);
+    for (int i = 0; i < w; ++i) BCK(cudaStreamCreateWithFlags(&b->lanes[i], cudaStreamNonBlocking));
+    for (auto& e : b->ev) BCK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    b->width = w;
+    return FGPE_OK;
+}
+
+// Capture nsteps of every instance as parallel branches (instance i runs on
+// lane i % width) of one graph.
+int capture(fgpe_batch_t* b, int nsteps) {
+    drop_graph(b);
+    // states must be in the spectral work buffer before capture (prologue)
+    for (fgpe_t* h : b->inst) {
+        if (!h->has_state) return bfail(b, FGPE_E_STATE, "batch instance without a state");
+        if (h->p.dim >= 2 && !h->S_valid) {
+            DISPATCH(h, launch_row, h, ROW_FWD, nullptr);
+            BCK(cudaGetLastError());
+            h->S_valid = true;
+        }
+        BCK(cudaStreamSynchronize(h->st));
+    }
+    cudaGraph_t g;
+    BCK(cudaStreamBeginCapture(b->origin, cudaStreamCaptureModeThreadLocal));
+    BCK(cudaEventRecord(b->ev[0], b->origin));
+    for (int l = 0; l < b->width; ++l) BCK(cudaStreamWaitEvent(b->lanes[l], b->ev[0], 0));
+    for (size_t i = 0; i < b->inst.size(); ++i) {
+        fgpe_t* h = b->inst[i];
+        cudaStream_t keep = h->st;
+        const bool prof = h->prof;
+        h->st = b->lanes[i % b->width];
+        h->prof = false;
+        const int rc = fgpe_step_ex(h, nsteps, FGPE_STEP_DEFAULT);
+        h->st = keep;
+        h->prof = prof;
+        if (rc) { cudaGraph_t junk; cudaStreamEndCapture(b->origin, &junk); if (junk) cudaGraphDestroy(junk); return rc; }
+    }
+    for (int l = 0; l < b->width; ++l) {
+        BCK(cudaEventRecord(b->ev[1 + l], b->lanes[l]));
+        BCK(cudaStreamWaitEvent(b->origin, b->ev[1 + l], 0));
+    }
+    BCK(cudaStreamEndCapture(b->origin, &g));
+    cudaError_t e = cudaGraphInstantiate(&b->exec, g, 0);
+    cudaGraphDestroy(g);
+    BCK(e);
+    b->exec_steps = nsteps;
+    return FGPE_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int fgpe_batch_create(const fgpe_params* p, int count, fgpe_batch_t** out) {
+    fgpe_batch_t* b = nullptr;
+    if (!p || count < 1 || !out) return bfail(b, FGPE_E_ARG, "bad batch arguments");
+    b = new fgpe_batch_s();
+    for (int i = 0; i < count; ++i) {
+        fgpe_t* h = nullptr;
+        const int rc = fgpe_create(&p[i], &h);
+        if (rc) { fgpe_batch_destroy(b); return bfail(nullptr, rc, "instance " + std::to_string(i) + ": " + g_last_error); }
+        b->inst.push_back(h);
+    }
+    BCK(cudaStreamCreateWithFlags(&b->origin, cudaStreamNonBlocking));
+    int r = set_width(b, std::min(count, 64));
+    if (r) return r;
+    b->ksteps = 16;
+    *out = b;
+    return FGPE_OK;
+}
+
+int fgpe_batch_destroy(fgpe_batch_t* b) {
+    if (!b) return FGPE_OK;
+    if (b->origin) cudaStreamSynchronize(b->origin);
+    drop_graph(b);
+    for (cudaStream_t s : b->lanes) cudaStreamDestroy(s);
+    for (cudaEvent_t e : b->ev) cudaEventDestroy(e);
+    if (b->origin) cudaStreamDestroy(b->origin);
+    for (fgpe_t* h : b->inst) fgpe_destroy(h);
+    delete b;
+    return FGPE_OK;
+}
+
+int fgpe_batch_size(const fgpe_batch_t* b) { return b ? (int)b->inst.size() : 0; }
+
+int fgpe_batch_instance(fgpe_batch_t* b, int i, fgpe_t** h) {
+    if (!b || !h || i < 0 || i >= (int)b->inst.size()) return bfail(b, FGPE_E_ARG, "bad instance index");
+    *h = b->inst[i];
+    return FGPE_OK;
+}
+
+const char* fgpe_batch_last_error(const fgpe_batch_t* b) { return b ? b->msg.c_str() : g_last_error.c_str(); }
+
+int fgpe_batch_config(fgpe_batch_t* b, int width, int steps_per_graph) {
+    if (!b) return bfail(b, FGPE_E_ARG, "null batch");
+    if (width > 0) { int r = set_width(b, width); if (r) return r; }
+    if (steps_per_graph > 0 && steps_per_graph != b->ksteps) { b->ksteps = steps_per_graph; drop_graph(b); }
+    return FGPE_OK;
+}
+
+int fgpe_batch_step(fgpe_batch_t* b, int nsteps) {
+    if (!b) return bfail(b, FGPE_E_ARG, "null batch");
+    // wait for work queued on the instances' own streams (set_state etc.)
+    for (fgpe_t* h : b->inst) BCK(cudaStreamSynchronize(h->st));
+    int left = nsteps;
+    while (left > 0) {
+        int k = std::min(left, b->ksteps);
+        if (k == 1 && left > 1) k = 2;
+        if (k == 1) {
+            // a single step keeps the one-step CONV semantics: run eagerly
+            for (size_t i = 0; i < b->inst.size(); ++i) {
+                fgpe_t* h = b->inst[i];
+                cudaStream_t keep = h->st;
+                h->st = b->lanes[i % b->width];
+                const int rc = fgpe_step_ex(h, 1, FGPE_STEP_DEFAULT);
+                h->st = keep;
+                if (rc) return rc;
+            }
+            for (int l = 0; l < b->width; ++l) BCK(cudaStreamSynchronize(b->lanes[l]));
+            left -= 1;
+            continue;
+        }
+        if (!b->exec || b->exec_steps != k) { int r = capture(b, k); if (r) return r; }
+        BCK(cudaGraphLaunch(b->exec, b->origin));
+        for (fgpe_t* h : b->inst) h->launches += (long long)k * (h->p.dim == 1 ? 1 : (h->p.dim == 2 ? 2 : 4));
+        left -= k;
+    }
+    BCK(cudaStreamSynchronize(b->origin));
+    return FGPE_OK;
+}
+
+// Observables of every instance: out[i*OBS] = en, mz, conv (if requested and
+// available, else -1), then mu[M], rms[M], norm[M] (stride 3+3*M).
+int fgpe_batch_observables(fgpe_batch_t* b, double* out, int with_conv) {
+    if (!b || !out) return bfail(b, FGPE_E_ARG, "null argument");
+    const int n = (int)b->inst.size();
+    size_t off = 0;
+    for (int i = 0; i < n; ++i) {
+        fgpe_t* h = b->inst[i];
+        const int ms = h->ms;
+        double* o = out + off;
+        off += 3 + 3 * ms;
+        int r = fgpe_observables(h, &o[0], o + 3, &o[1], o + 3 + ms);
+        if (r) return r;
+        r = fgpe_norms(h, o + 3 + 2 * ms);
+        if (r) return r;
+        o[2] = -1.0;
+        if (with_conv && h->prev_valid) { r = fgpe_conv(h, &o[2]); if (r) return r; }
+    }
+    return FGPE_OK;
+}
+
+// Autotuner: times candidate (kernel family per grid-size class, branch
+// width, steps per graph) settings on the batch itself and keeps the fastest.
+// The instances' states are saved before and restored after the trials, so
+// tuning does not advance the physics.  The result is remembered in a small
+// text cache (one line per batch signature) when cache_path is given.
+int fgpe_batch_autotune(fgpe_batch_t* b, int trial_steps, const char* cache_path) {
+    if (!b) return bfail(b, FGPE_E_ARG, "null batch");
+    const int n = (int)b->inst.size();
+    if (trial_steps < 2) trial_steps = 8;
+    // signature: device, precision, spin and the sorted grid sizes
+    cudaDeviceProp prop;
+    int dev = 0; cudaGetDevice(&dev); cudaGetDeviceProperties(&prop, dev);
+    std::vector<std::string> sizes;
+    for (fgpe_t* h : b->inst)
+        sizes.push_back(std::to_string(h->p.nx) + "x" + std::to_string(h->p.ny) + "x" + std::to_string(h->p.nz) + "s" +
+                        std::to_string(h->p.spin) + (h->fp32 ? "f" : "d"));
+    std::vector<std::string> classes = sizes;
+    std::sort(classes.begin(), classes.end());
+    classes.erase(std::unique(classes.begin(), classes.end()), classes.end());
+    std::string sig = std::string(prop.name) + "|" + std::to_string(n);
+    for (auto& c : classes) sig += "|" + c + ":" + std::to_string(std::count(sizes.begin(), sizes.end(), c));
+    for (char& ch : sig) if (ch == ' ') ch = '_';
+    // cached?
+    if (cache_path) {
+        FILE* f = fopen(cache_path, "r");
+        if (f) {
+            char line[8192];
+            while (fgets(line, sizeof line, f)) {
+                std::string l(line);
+                if (l.compare(0, sig.size() + 1, sig + " ") != 0) continue;
+                int w = 0, k = 0;
+                char fam[4096] = {0};
+                if (sscanf(l.c_str() + sig.size() + 1, "%d %d %4095s", &w, &k, fam) == 3) {
+                    fclose(f);
+                    std::string fs(fam);
+                    for (size_t ci = 0; ci < classes.size() && ci < fs.size(); ++ci)
+                        for (int i = 0; i < n; ++i)
+                            if (sizes[i] == classes[ci]) fgpe_set_kernels(b->inst[i], fs[ci] == 'g' ? FGPE_KERNELS_GENERIC : FGPE_KERNELS_AUTO);
+                    return fgpe_batch_config(b, w, k);
+                }
+            }
+            fclose(f);
+        }
+    }
+    // save states (spectral buffer or real-space copy, plus the info vector)
+    std::vector<void*> save(n, nullptr), save_info(n, nullptr);
+    std::vector<char> flags(3 * n);
+    for (int i = 0; i < n; ++i) {
+        fgpe_t* h = b->inst[i];
+        BCK(cudaStreamSynchronize(h->st));
+        const size_t bytes = (size_t)h->npts * h->ms * h->cs;
+        BCK(cudaMalloc(&save[i], 2 * bytes));
+        BCK(cudaMalloc(&save_info[i], 2 * INFO_LEN * sizeof(double)));
+        BCK(cudaMemcpy(save[i], h->S, bytes, cudaMemcpyDeviceToDevice));
+        BCK(cudaMemcpy((char*)save[i] + bytes, h->psi, bytes, cudaMemcpyDeviceToDevice));
+        BCK(cudaMemcpy(save_info[i], h->info, 2 * INFO_LEN * sizeof(double), cudaMemcpyDeviceToDevice));
+        flags[3 * i] = h->S_valid; flags[3 * i + 1] = h->psi_valid; flags[3 * i + 2] = h->prev_valid;
+    }
+    cudaEvent_t t0, t1;
+    BCK(cudaEventCreate(&t0));
+    BCK(cudaEventCreate(&t1));
+    auto timed = [&](int w, int k, double* ms) -> int {
+        int r = fgpe_batch_config(b, w, k);
+        if (r) return r;
+        r = fgpe_batch_step(b, k);          // warm-up, includes capture
+        if (r) return r;
+        BCK(cudaEventRecord(t0, b->origin));
+        r = fgpe_batch_step(b, trial_steps);
+        if (r) return r;
+        BCK(cudaEventRecord(t1, b->origin));
+        BCK(cudaEventSynchronize(t1));
+        float f = 0;
+        BCK(cudaEventElapsedTime(&f, t0, t1));
+        *ms = f / trial_steps;
+        return FGPE_OK;
+    };
+    // 1) kernel family per size class (fast where available), at a default shape
+    std::string fam(classes.size(), 'f');
+    double best_ms = 1e30;
+    for (size_t ci = 0; ci < classes.size(); ++ci) {
+        double tms[2] = {1e30, 1e30};
+        for (int opt = 0; opt < 2; ++opt) {
+            for (int i = 0; i < n; ++i)
+                if (sizes[i] == classes[ci]) fgpe_set_kernels(b->inst[i], opt ? FGPE_KERNELS_GENERIC : FGPE_KERNELS_AUTO);
+            int r = timed(std::min(n, 64), 8, &tms[opt]);
+            if (r) return r;
+        }
+        const int pick = tms[1] < tms[0] ? 1 : 0;
+        fam[ci] = pick ? 'g' : 'f';
+        for (int i = 0; i < n; ++i)
+            if (sizes[i] == classes[ci]) fgpe_set_kernels(b->inst[i], pick ? FGPE_KERNELS_GENERIC : FGPE_KERNELS_AUTO);
+        best_ms = std::min(tms[0], tms[1]);
+    }
+    // 2) branch width and steps per graph
+    int bw = std::min(n, 64), bk = 8;
+    const int widths[] = {4, 16, 32, 64, 128, 256, 512};
+    const int ks[] = {4, 8, 32};
+    for (int w : widths) {
+        if (w > n) continue;
+        for (int k : ks) {
+            double ms = 0;
+            int r = timed(w, k, &ms);
+            if (r) return r;
+            if (ms < best_ms) { best_ms = ms; bw = w; bk = k; }
+        }
+    }
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    // restore the states
+    for (int i = 0; i < n; ++i) {
+        fgpe_t* h = b->inst[i];
+        const size_t bytes = (size_t)h->npts * h->ms * h->cs;
+        BCK(cudaMemcpy(h->S, save[i], bytes, cudaMemcpyDeviceToDevice));
+        BCK(cudaMemcpy(h->psi, (char*)save[i] + bytes, bytes, cudaMemcpyDeviceToDevice));
+        BCK(cudaMemcpy(h->info, save_info[i], 2 * INFO_LEN * sizeof(double), cudaMemcpyDeviceToDevice));
+        h->S_valid = flags[3 * i]; h->psi_valid = flags[3 * i + 1]; h->prev_valid = flags[3 * i + 2];
+        cudaFree(save[i]);
+        cudaFree(save_info[i]);
+    }
+    int r = fgpe_batch_config(b, bw, bk);
+    if (r) return r;
+    if (cache_path) {
+        FILE* f = fopen(cache_path, "a");
+        if (f) { fprintf(f, "%s %d %d %s %.6f\n", sig.c_str(), bw, bk, fam.c_str(), best_ms); fclose(f); }
+    }
+    return FGPE_OK;
+}
+
+int fgpe_batch_tuning(const fgpe_batch_t* b, int* width, int* steps_per_graph) {
+    if (!b) return FGPE_E_ARG;
+    if (width) *width = b->width;
+    if (steps_per_graph) *steps_per_graph = b->ksteps;
+    return FGPE_OK;
+}
 
 int fgpe_kernel_launches(fgpe_t* h, long long* count) {
     if (!h || !count) return fail(h, FGPE_E_ARG, "null argument");

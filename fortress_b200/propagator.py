@@ -31,34 +31,44 @@ def _dp(a):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
 
 
+def make_params(dim, spin, n, d, dt, imag_time, tau, gamma=(0.0, 0.0, 0.0),
+                alpha=(1.0, 1.0, 1.0), precision="fp64", kernels="auto", mag=0.0):
+    """Fill an fgpe_params structure (include/fgpe.h)."""
+    p = _abi.Params()
+    n = list(n) + [1] * (3 - len(n))
+    d = list(d) + [1.0] * (3 - len(d))
+    g = list(gamma) + [0.0] * (3 - len(gamma))
+    t = list(tau) + [0.0] * (3 - len(tau))
+    p.dim, p.spin = int(dim), int(spin)
+    p.nx, p.ny, p.nz = (int(v) for v in n)
+    p.dx, p.dy, p.dz = (float(v) for v in d)
+    p.dt = float(dt)
+    p.imag_time = int(bool(imag_time))
+    for i in range(3):
+        p.tau[i] = float(t[i])
+        p.gamma[i] = float(g[i])
+        p.alpha[i] = float(alpha[i])
+    p.precision = _abi.FGPE_FP32 if str(precision).lower() in ("fp32", "float32", "1") else _abi.FGPE_FP64
+    p.kernels = {"auto": 0, "generic": 1, "fast-row": 2, "fast-col": 3}[kernels]
+    p.mag = float(mag)
+    return p
+
+
 class Propagator:
     def __init__(self, dim, spin, n, d, dt, imag_time, tau, gamma=(0.0, 0.0, 0.0),
-                 alpha=(1.0, 1.0, 1.0), precision="fp64", kernels="auto", mag=0.0):
+                 alpha=(1.0, 1.0, 1.0), precision="fp64", kernels="auto", mag=0.0, _handle=None, _owner=None):
         L = _abi.load()
-        p = _abi.Params()
-        n = list(n) + [1] * (3 - len(n))
-        d = list(d) + [1.0] * (3 - len(d))
-        g = list(gamma) + [0.0] * (3 - len(gamma))
-        t = list(tau) + [0.0] * (3 - len(tau))
-        p.dim, p.spin = int(dim), int(spin)
-        p.nx, p.ny, p.nz = (int(v) for v in n)
-        p.dx, p.dy, p.dz = (float(v) for v in d)
-        p.dt = float(dt)
-        p.imag_time = int(bool(imag_time))
-        for i in range(3):
-            p.tau[i] = float(t[i])
-            p.gamma[i] = float(g[i])
-            p.alpha[i] = float(alpha[i])
-        p.precision = _abi.FGPE_FP32 if str(precision).lower() in ("fp32", "float32", "1") else _abi.FGPE_FP64
-        p.kernels = {"auto": 0, "generic": 1, "fast-row": 2, "fast-col": 3}[kernels]
-        p.mag = float(mag)
         self.params = p
         self.dim, self.spin, self.ms = p.dim, p.spin, 2 * p.spin + 1
         self.shape = (p.nx, p.ny if p.dim >= 2 else 1, p.nz if p.dim >= 3 else 1)
+        self._L = L
+        self._owner = _owner
+        if _handle is not None:          # an instance owned by a Batch
+            self._h = _handle
+            return
         h = ctypes.c_void_p()
         check(L.fgpe_create(ctypes.byref(p), ctypes.byref(h)))
         self._h = h
-        self._L = L
 
     @classmethod
     def from_config(cls, cfg, precision="fp64"):
@@ -66,7 +76,8 @@ class Propagator:
 
     def close(self):
         if getattr(self, "_h", None):
-            self._L.fgpe_destroy(self._h)
+            if self._owner is None:
+                self._L.fgpe_destroy(self._h)
             self._h = None
 
     def __del__(self):
@@ -173,6 +184,9 @@ class Propagator:
         n = (ctypes.c_longlong * 4)()
         self._ck(self._L.fgpe_profile_read(self._h, _dp(ms), n, int(reset)))
         return ms, np.array(list(n))
+
+    def set_kernels(self, kernels):
+        self._ck(self._L.fgpe_set_kernels(self._h, {"auto": 0, "generic": 1, "fast-row": 2, "fast-col": 3}[kernels]))
 
     def kernel_launches(self):
         c = ctypes.c_longlong()

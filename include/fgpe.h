@@ -143,6 +143,39 @@ int fgpe_norms_async(fgpe_t *h, double *dst);
 int fgpe_profile_enable(fgpe_t *h, int on);
 int fgpe_profile_read(fgpe_t *h, double *ms, long long *n, int reset);
 
+/* ------------------------------------------------------------------ batches
+ * Many independent instances (ragged grid sizes, per-instance parameters)
+ * advanced together: every instance's split steps are captured as a parallel
+ * branch of one CUDA graph (instance i on branch i % width) and the graph is
+ * replayed with one launch per steps_per_graph steps.  The reference has no
+ * counterpart (it runs one configuration per process); this is the sweep
+ * launcher over parameter points.  Instances are ordinary handles: set their
+ * states and read their observables through fgpe_batch_instance(). */
+typedef struct fgpe_batch_s fgpe_batch_t;
+int fgpe_batch_create(const fgpe_params *p, int count, fgpe_batch_t **out);
+int fgpe_batch_destroy(fgpe_batch_t *b);
+int fgpe_batch_size(const fgpe_batch_t *b);
+int fgpe_batch_instance(fgpe_batch_t *b, int i, fgpe_t **h);
+const char *fgpe_batch_last_error(const fgpe_batch_t *b);
+/* width: concurrent graph branches (<= count); steps_per_graph: steps
+ * captured per graph launch (>= 2).  Non-positive values keep the setting. */
+int fgpe_batch_config(fgpe_batch_t *b, int width, int steps_per_graph);
+int fgpe_batch_step(fgpe_batch_t *b, int nsteps);
+/* For every instance i in order, 3+3*M_i doubles: EN, MZ, CONV (max|dphi|
+ * of the last step, or -1), MU[M_i], RMS[M_i], NORM[M_i]. */
+int fgpe_batch_observables(fgpe_batch_t *b, double *out, int with_conv);
+
+/* Autotuner: times kernel family per grid-size class, branch width and
+ * steps per graph on the batch itself (states saved and restored) and keeps
+ * the fastest; cache_path (may be NULL) remembers the choice per batch
+ * signature.  fgpe_batch_tuning reports the current width and steps. */
+int fgpe_batch_autotune(fgpe_batch_t *b, int trial_steps, const char *cache_path);
+int fgpe_batch_tuning(const fgpe_batch_t *b, int *width, int *steps_per_graph);
+
+/* Switch one handle between the size-specialised and the generic kernels
+ * (same data layout, so this can happen between any two calls). */
+int fgpe_set_kernels(fgpe_t *h, int kernels);
+
 /* Library / device information. */
 int fgpe_version(void);
 int fgpe_device_ok(void);                /* 1 if an sm_100 device is usable */
