@@ -58,6 +58,7 @@ class Propagator:
     def __init__(self, dim, spin, n, d, dt, imag_time, tau, gamma=(0.0, 0.0, 0.0),
                  alpha=(1.0, 1.0, 1.0), precision="fp64", kernels="auto", mag=0.0, _handle=None, _owner=None):
         L = _abi.load()
+        p = make_params(dim, spin, n, d, dt, imag_time, tau, gamma, alpha, precision, kernels, mag)
         self.params = p
         self.dim, self.spin, self.ms = p.dim, p.spin, 2 * p.spin + 1
         self.shape = (p.nx, p.ny if p.dim >= 2 else 1, p.nz if p.dim >= 3 else 1)
