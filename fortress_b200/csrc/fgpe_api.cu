@@ -19,6 +19,8 @@
 #include "../../include/fgpe.h"
 #include "fgpe_kernels.cuh"
 #include "fgpe_fast.cuh"
+#include "fno_kernels.cuh"
+#include "../../include/fno.h"
 
 using namespace fgpe;
 
@@ -1312,6 +1314,73 @@ int fgpe_kernel_launches(fgpe_t* h, long long* count) {
     if (!h || !count) return fail(h, FGPE_E_ARG, "null argument");
     *count = h->launches;
     return FGPE_OK;
+}
+
+}  // extern "C"
+
+// ================================================================ FNO ABI
+extern "C" {
+
+static int fno_ck(cudaError_t e) {
+    if (e != cudaSuccess) { g_last_error = cudaGetErrorString(e); return FGPE_E_CUDA; }
+    return FGPE_OK;
+}
+static unsigned fno_grid(long long n) { long long g = (n + 255) / 256; return (unsigned)std::min<long long>(g, 148LL * 32); }
+
+int fno_gemm(int batch, int M, int N, int K, float alpha, const void* A, int a_bf16, long long sAb, long long sAi,
+             long long sAk, const float* B, long long sBb, long long sBk, long long sBj, float beta, float* C,
+             long long sCb, long long sCi, long long sCj, void* stream) {
+    if (batch <= 0 || M <= 0 || N <= 0 || K <= 0) return FGPE_E_ARG;
+    if (batch > 65535) return FGPE_E_ARG;
+    dim3 grid((N + 63) / 64, (M + 63) / 64, batch);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (a_bf16)
+        fno::k_gemm<__nv_bfloat16><<<grid, 256, 0, st>>>(M, N, K, alpha, (const __nv_bfloat16*)A, sAb, sAi, sAk, B, sBb,
+                                                         sBk, sBj, beta, C, sCb, sCi, sCj);
+    else
+        fno::k_gemm<float><<<grid, 256, 0, st>>>(M, N, K, alpha, (const float*)A, sAb, sAi, sAk, B, sBb, sBk, sBj, beta, C,
+                                                 sCb, sCi, sCj);
+    return fno_ck(cudaGetLastError());
+}
+
+int fno_bias_act(float* z, float* h, const float* bias, long long C, long long S, long long n, int act, void* stream) {
+    fno::k_bias_act<<<fno_grid(n), 256, 0, (cudaStream_t)stream>>>(z, h, bias, C, S, n, act);
+    return fno_ck(cudaGetLastError());
+}
+
+int fno_act_bwd(float* dz, const float* dh, const float* z, long long n, void* stream) {
+    fno::k_act_bwd<<<fno_grid(n), 256, 0, (cudaStream_t)stream>>>(dz, dh, z, n);
+    return fno_ck(cudaGetLastError());
+}
+
+int fno_channel_sum(float* out, const float* x, long long B, long long C, long long S, float beta, void* stream) {
+    fno::k_channel_sum<<<(unsigned)C, 256, 0, (cudaStream_t)stream>>>(out, x, B, C, S, beta);
+    return fno_ck(cudaGetLastError());
+}
+
+int fno_axpy(float* y, const float* x, float a, long long n, void* stream) {
+    fno::k_axpy<<<fno_grid(n), 256, 0, (cudaStream_t)stream>>>(y, x, a, n);
+    return fno_ck(cudaGetLastError());
+}
+
+int fno_mse(const float* out, const float* target, float* dout, double* loss_dev, double* scratch, long long n,
+            void* stream) {
+    fno::k_mse<<<256, 256, 0, (cudaStream_t)stream>>>(out, target, dout, scratch, n);
+    fno::k_sum_parts<<<1, 32, 0, (cudaStream_t)stream>>>(scratch, 256, 1.0 / (double)n, loss_dev);
+    return fno_ck(cudaGetLastError());
+}
+
+int fno_adam(float* w, void* w_bf16, const float* g, float* m, float* v, long long n, float lr, float beta1,
+             float beta2, float eps, int t, void* stream) {
+    const float c1 = 1.f - powf(beta1, (float)t), c2 = 1.f - powf(beta2, (float)t);
+    fno::k_adam<<<fno_grid(n), 256, 0, (cudaStream_t)stream>>>(w, (__nv_bfloat16*)w_bf16, g, m, v, n, lr, beta1, beta2,
+                                                              eps, c1, c2);
+    return fno_ck(cudaGetLastError());
+}
+
+int fno_to_bf16(const float* x, void* y, long long n, void* stream) {
+    fno::k_to_bf16<<<fno_grid(n), 256, 0, (cudaStream_t)stream>>>(x, (__nv_bfloat16*)y, n);
+    return fno_ck(cudaGetLastError());
 }
 
 }  // extern "C"

@@ -49,8 +49,9 @@ def compare(name, cfg, steps):
     phi = _guess(p64)
     a, b = F.Propagator(**p64), F.Propagator(**p32)
     a.set_state(phi); b.set_state(phi)
-    if cfg.switch_im:
-        a.normt(); b.normt()
+    # start both from the unit-norm state: a real-time run of the reference
+    # continues a normalised imaginary-time solution
+    a.normt(); b.normt()
     a.step(steps); b.step(steps)
     ea, mua, mza, ra = a.observables()
     eb, mub, mzb, rb = b.observables()

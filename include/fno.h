@@ -1,0 +1,44 @@
+/*
+ * fno.h -- C ABI of the kernels that train and evaluate the learned initial
+ * guess (a Fourier neural operator mapping physical parameters to a spinor).
+ * No counterpart in the reference (FORTRESS starts from fixed analytic
+ * guesses, cgpe1d.f90:707-790); the guess it produces feeds fgpe_set_state.
+ *
+ * All pointers are device pointers; all calls are asynchronous on `stream`
+ * (cudaStream_t, NULL = legacy default stream) and return 0 or an FGPE_E_*
+ * code.  Tensors are float32 unless stated; weight operands may be bfloat16.
+ */
+#ifndef FNO_H
+#define FNO_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Batched strided GEMM with FP32 accumulation:
+ *   C[b](i,j) = alpha * sum_k A[b](i,k) B[b](k,j) + beta * C[b](i,j)
+ * with A[b](i,k) at A + b*sAb + i*sAi + k*sAk (elements; likewise B, C).
+ * a_bf16 != 0: A holds bfloat16 values. */
+int fno_gemm(int batch, int M, int N, int K, float alpha, const void *A, int a_bf16, long long sAb,
+             long long sAi, long long sAk, const float *B, long long sBb, long long sBk, long long sBj,
+             float beta, float *C, long long sCb, long long sCi, long long sCj, void *stream);
+/* z[b,c,s] += bias[c] (bias may be NULL); h = GELU(z) if act else z (h may be NULL). */
+int fno_bias_act(float *z, float *h, const float *bias, long long C, long long S, long long n, int act, void *stream);
+/* dz = dh * GELU'(z) */
+int fno_act_bwd(float *dz, const float *dh, const float *z, long long n, void *stream);
+/* out[c] = beta*out[c] + sum over b and s of x[b,c,s] */
+int fno_channel_sum(float *out, const float *x, long long B, long long C, long long S, float beta, void *stream);
+/* y += a*x */
+int fno_axpy(float *y, const float *x, float a, long long n, void *stream);
+/* loss = mean((out-target)^2) into *loss_dev (double, device); dout = d loss/d out (may be NULL);
+ * scratch: >= 256 doubles of device memory. */
+int fno_mse(const float *out, const float *target, float *dout, double *loss_dev, double *scratch, long long n, void *stream);
+/* One Adam step (bias-corrected, step t >= 1) on FP32 master weights w;
+ * w_bf16 (may be NULL) receives the bfloat16 copy. */
+int fno_adam(float *w, void *w_bf16, const float *g, float *m, float *v, long long n, float lr, float beta1,
+             float beta2, float eps, int t, void *stream);
+int fno_to_bf16(const float *x, void *y, long long n, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FNO_H */
