@@ -178,6 +178,22 @@ def run_cpu(phi, cfg, steps, warmup, budget_s=None):
     return 512 * 512 * done / el, done, el, O.num_threads()
 
 
+def capture(args):
+    """The headline step alone: warmup + steps split steps of the 512^2 spin-2
+    real-time case from the noisy Gaussian guess, for ncu launch lists and
+    per-kernel captures (-k regex:k_row_fast / k_col_fast)."""
+    import numpy as np
+    import fortress_b200 as F
+    cfg = workload_config(WORKLOAD["gamma"])
+    prop = F.Propagator(**cfg.params(args.precision))
+    prop.set_state(add_noise(gaussian_guess(cfg)))
+    prop.step(args.warmup + args.steps, snapshot=False)
+    n = prop.normc()
+    assert np.all(np.isfinite(n))
+    print(json.dumps({"capture": WORKLOAD["name"], "precision": args.precision,
+                      "steps": args.warmup + args.steps, "norm": float(n.sum())}))
+
+
 # -------------------------------------------------------------------- main
 def main():
     ap = argparse.ArgumentParser()
@@ -192,8 +208,13 @@ def main():
     ap.add_argument("--workload", default="q2d", choices=["q2d", "3d", "sweep"],
                     help="q2d: 512^2 spin-2 real time (headline); 3d: 256^3 spin-1 imaginary time; "
                          "sweep: 512 ragged q2D spin-1 instances in one batched graph launch")
+    ap.add_argument("--capture", action="store_true",
+                    help="run only the workload's step kernels (warmup + steps launches of each, on the "
+                         "unrelaxed guess, no timing, no other work) for profiler captures")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.capture:
+        return capture(args)
     if args.workload != "q2d" and args.impl == "ours":
         return other_workload(args)
 
