@@ -37,7 +37,7 @@ EXPORTS = (
     "fgpe_kernel_launches", "fgpe_norms_async", "fgpe_profile_enable", "fgpe_profile_read",
     "fgpe_batch_create", "fgpe_batch_destroy", "fgpe_batch_size", "fgpe_batch_instance",
     "fgpe_batch_last_error", "fgpe_batch_config", "fgpe_batch_step", "fgpe_batch_observables",
-    "fgpe_batch_autotune", "fgpe_batch_tuning", "fgpe_set_kernels",
+    "fgpe_batch_autotune", "fgpe_batch_tuning", "fgpe_set_kernels", "fgpe_normc_noalloc",
 )
 
 
@@ -103,6 +103,8 @@ def load():
         "fgpe_batch_autotune": ([vp, ip, ctypes.c_char_p], ip),
         "fgpe_batch_tuning": ([vp, ctypes.POINTER(ip), ctypes.POINTER(ip)], ip),
         "fgpe_set_kernels": ([vp, ip], ip),
+        "fgpe_normc_noalloc": ([ip, ip, ip, ip, ip, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                vp, vp, vp], ip),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

@@ -13,6 +13,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1384,3 +1385,136 @@ int fno_to_bf16(const float* x, void* y, long long n, void* stream) {
 }
 
 }  // extern "C"
+
+// ===================================================== NORMC without allocation
+// fgpe_normc_noalloc: NORMC of a caller's device-resident spinor with no
+// handle and no allocation of any kind.  Its only scratch is the file-scope
+// array below (per-line Simpson integrals plus the last-block counter).  The
+// address is looked up once per device with that device current, on the
+// first call made there; afterwards a call only launches one kernel.
+// The counter must be zero when a call starts: it is zero when the module is
+// loaded and the last block of every call sets it back to zero.  The line
+// values need no initial contents (every call writes all it reads).  Two calls
+// in flight at once on one device share the scratch and race.
+namespace {
+
+constexpr long long kNoAllocMaxValues = 262144;  // lines x components (2 MiB)
+
+struct NoAllocScratch {
+    double line[kNoAllocMaxValues];
+    unsigned int counter;
+};
+static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
+
+// Weight of node i (0-based) of the reference's SIMPSON (simpson.f90:4-21) on
+// an even number n >= 8 of nodes: Simpson 1/3 over nodes 1..n-3 and 3/8 over
+// the last four (1-based f): f=1 -> h/3; even f <= n-4 -> 4h/3; odd 3 <= f <=
+// n-5 -> 2h/3; f=n-3 -> h/3 + 3h/8; f=n-2, n-1 -> 9h/8; f=n -> 3h/8.
+__device__ __forceinline__ double noalloc_simpson_w(int i, int n, double h) {
+    if (n == 1) return 1.0;
+    const int f = i + 1;
+    if (f == 1) return h / 3.0;
+    if (f == n) return 3.0 * h / 8.0;
+    if (f == n - 1 || f == n - 2) return 9.0 * h / 8.0;
+    if (f == n - 3) return h / 3.0 + 3.0 * h / 8.0;
+    return (f % 2 == 0) ? 4.0 * h / 3.0 : 2.0 * h / 3.0;
+}
+
+// One warp per x line: Simpson integral of |phi_m|^2 along x into the
+// scratch; the last block to finish integrates the lines over y and z with
+// the same weights in a fixed order and restores the counter.
+template <int MS>
+__global__ void __launch_bounds__(256)
+k_normc_noalloc(const double2* __restrict__ phi, int nx, int ny, long long nlines, long long npts, double dx,
+                double dy, double dz, int nz, NoAllocScratch* s, double* __restrict__ norm) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (long long l = (long long)blockIdx.x * 8 + warp; l < nlines; l += (long long)gridDim.x * 8) {
+        const double2* row = phi + l * nx;
+#pragma unroll
+        for (int m = 0; m < MS; ++m) {
+            double acc = 0.0;
+            for (int i = lane; i < nx; i += 32) {
+                const double2 v = row[(size_t)m * npts + i];
+                acc += noalloc_simpson_w(i, nx, dx) * (v.x * v.x + v.y * v.y);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+            if (lane == 0) s->line[l * MS + m] = acc;
+        }
+    }
+    __threadfence();
+    __syncthreads();
+    __shared__ unsigned int last;
+    if (threadIdx.x == 0) last = (atomicAdd(&s->counter, 1u) == gridDim.x - 1);
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    __shared__ double red[256];
+    for (int m = 0; m < MS; ++m) {
+        double acc = 0.0;
+        for (long long l = threadIdx.x; l < nlines; l += 256) {
+            const int j = (int)(l % ny), k = (int)(l / ny);
+            acc += noalloc_simpson_w(j, ny, dy) * noalloc_simpson_w(k, nz, dz) * __ldcg(&s->line[l * MS + m]);
+        }
+        red[threadIdx.x] = acc;
+        __syncthreads();
+        for (int o = 128; o > 0; o >>= 1) {
+            if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) norm[m] = red[0];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) s->counter = 0u;
+}
+
+std::mutex g_noalloc_mu;
+NoAllocScratch* g_noalloc_ptr[64] = {};
+
+}  // namespace
+
+extern "C" int fgpe_normc_noalloc(int dim, int spin, int nx, int ny, int nz, double dx, double dy, double dz,
+                                  const void* phi_dev, double* norm_dev, void* stream) {
+    if (!phi_dev || !norm_dev) return fail(nullptr, FGPE_E_ARG, "null argument");
+    if (dim < 1 || dim > 3) return fail(nullptr, FGPE_E_ARG, "dim must be 1, 2 or 3");
+    if (spin != 1 && spin != 2) return fail(nullptr, FGPE_E_ARG, "spin must be 1 or 2");
+    if (dim < 2) ny = 1;
+    if (dim < 3) nz = 1;
+    const int n[3] = {nx, ny, nz};
+    const double d[3] = {dx, dy, dz};
+    for (int a = 0; a < dim; ++a) {
+        if (n[a] < 8 || n[a] % 2) return fail(nullptr, FGPE_E_ARG, "every grid axis needs an even number >= 8 of points");
+        if (!(d[a] > 0.0)) return fail(nullptr, FGPE_E_ARG, "grid spacings must be positive");
+    }
+    const int ms = 2 * spin + 1;
+    const long long nlines = (long long)ny * nz;
+    if (nlines * ms > kNoAllocMaxValues)
+        return fail(nullptr, FGPE_E_ARG,
+                    "grid too large for the static scratch: (ny*nz lines) x components = " +
+                        std::to_string(nlines * ms) + " exceeds " + std::to_string(kNoAllocMaxValues));
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return fail(nullptr, FGPE_E_CUDA, cudaGetErrorString(e));
+    if (dev < 0 || dev >= 64) return fail(nullptr, FGPE_E_ARG, "device ordinal beyond 63");
+    NoAllocScratch* s = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_noalloc_mu);
+        if (!g_noalloc_ptr[dev]) {
+            void* p = nullptr;
+            e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+            if (e != cudaSuccess) return fail(nullptr, FGPE_E_CUDA, std::string("scratch lookup: ") + cudaGetErrorString(e));
+            g_noalloc_ptr[dev] = (NoAllocScratch*)p;
+        }
+        s = g_noalloc_ptr[dev];
+    }
+    const long long npts = nlines * nx;
+    const unsigned grid = (unsigned)std::min<long long>((nlines + 7) / 8, 148LL * 8);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (ms == 3)
+        k_normc_noalloc<3><<<grid, 256, 0, st>>>((const double2*)phi_dev, nx, ny, nlines, npts, dx, dy, dz, nz, s, norm_dev);
+    else
+        k_normc_noalloc<5><<<grid, 256, 0, st>>>((const double2*)phi_dev, nx, ny, nlines, npts, dx, dy, dz, nz, s, norm_dev);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(nullptr, FGPE_E_CUDA, cudaGetErrorString(e));
+    return FGPE_OK;
+}

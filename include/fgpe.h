@@ -176,6 +176,24 @@ int fgpe_batch_tuning(const fgpe_batch_t *b, int *width, int *steps_per_graph);
  * (same data layout, so this can happen between any two calls). */
 int fgpe_set_kernels(fgpe_t *h, int kernels);
 
+/* NORMC of a spinor the caller already holds on the device, with no handle
+ * and no allocation of any kind: for callers that may not allocate device
+ * memory, such as a host code whose device memory is reserved up front by
+ * its own pool or a solver that must not synchronise the device in the
+ * middle of a run (cudaMalloc/cudaFree synchronise).  No counterpart in the
+ * reference (NORMC, cgpe1d.f90:957-993, works on its module state).
+ *   phi_dev: complex128, the PHI layout of fgpe_set_state; norm_dev: 2*spin+1
+ *   doubles of device memory; stream: cudaStream_t (NULL = legacy default).
+ * Asynchronous: the result is in norm_dev once the stream reaches it.
+ * Limits: every used axis an even number >= 8 of points (the reference's
+ * Simpson rule), and (ny*nz lines) x (2*spin+1) <= 262144, the size of the
+ * library's fixed 2 MiB scratch; larger grids return FGPE_E_ARG.  The first
+ * call on each device looks the scratch up (cudaGetSymbolAddress) with that
+ * device current; make it before any stream capture.  Calls on one device
+ * share the scratch: never have two in flight at once. */
+int fgpe_normc_noalloc(int dim, int spin, int nx, int ny, int nz, double dx, double dy, double dz,
+                       const void *phi_dev, double *norm_dev, void *stream);
+
 /* Library / device information. */
 int fgpe_version(void);
 int fgpe_device_ok(void);                /* 1 if an sm_100 device is usable */
