@@ -1384,6 +1384,19 @@ int fno_to_bf16(const float* x, void* y, long long n, void* stream) {
     return fno_ck(cudaGetLastError());
 }
 
+int fno_rbig_build(const float* rr, const float* ri, void* rbig, long long nmodes, int O, int C, void* stream) {
+    if (nmodes <= 0 || O <= 0 || C <= 0) return FGPE_E_ARG;
+    fno::k_rbig_build<<<fno_grid(nmodes * 4LL * O * C), 256, 0, (cudaStream_t)stream>>>(rr, ri, (__nv_bfloat16*)rbig,
+                                                                                        nmodes, O, C);
+    return fno_ck(cudaGetLastError());
+}
+
+int fno_rbig_fold(const float* drbig, float* drr, float* dri, long long nmodes, int O, int C, void* stream) {
+    if (nmodes <= 0 || O <= 0 || C <= 0) return FGPE_E_ARG;
+    fno::k_rbig_fold<<<fno_grid(nmodes * (long long)O * C), 256, 0, (cudaStream_t)stream>>>(drbig, drr, dri, nmodes, O, C);
+    return fno_ck(cudaGetLastError());
+}
+
 }  // extern "C"
 
 // ===================================================== NORMC without allocation

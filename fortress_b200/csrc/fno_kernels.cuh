@@ -167,4 +167,35 @@ __global__ void k_to_bf16(const float* x, __nv_bfloat16* y, long long n) {
         y[t] = __float2bfloat16(x[t]);
 }
 
+// Real block form of the per-mode complex channel mixing G = R H:
+//   Rbig[mode] = [[Rr, -Ri], [Ri, Rr]]   (2O x 2C), R stored [mode][O][C]
+__global__ void k_rbig_build(const float* rr, const float* ri, __nv_bfloat16* rb, long long nmodes, int O, int C) {
+    const long long n = nmodes * 4LL * O * C;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const long long mode = t / (4LL * O * C);
+        const int e = (int)(t % (4LL * O * C));
+        const int row = e / (2 * C), col = e % (2 * C);
+        const int po = row / O, o = row % O, pc = col / C, c = col % C;
+        const long long src = (mode * O + o) * C + c;
+        float v;
+        if (po == pc) v = rr[src];
+        else v = (po == 0) ? -ri[src] : ri[src];
+        rb[t] = __float2bfloat16(v);
+    }
+}
+
+// Gradient of the block form folded back: dRr = d00 + d11, dRi = d10 - d01.
+__global__ void k_rbig_fold(const float* drb, float* drr, float* dri, long long nmodes, int O, int C) {
+    const long long n = nmodes * (long long)O * C;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const long long mode = t / ((long long)O * C);
+        const int o = (int)((t / C) % O), c = (int)(t % C);
+        const float* d = drb + mode * 4LL * O * C;
+        const float d00 = d[(long long)o * 2 * C + c], d01 = d[(long long)o * 2 * C + C + c];
+        const float d10 = d[(long long)(O + o) * 2 * C + c], d11 = d[(long long)(O + o) * 2 * C + C + c];
+        drr[t] = d00 + d11;
+        dri[t] = d10 - d01;
+    }
+}
+
 }  // namespace fno

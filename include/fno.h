@@ -37,6 +37,11 @@ int fno_mse(const float *out, const float *target, float *dout, double *loss_dev
 int fno_adam(float *w, void *w_bf16, const float *g, float *m, float *v, long long n, float lr, float beta1,
              float beta2, float eps, int t, void *stream);
 int fno_to_bf16(const float *x, void *y, long long n, void *stream);
+/* Per-mode complex channel mixing in real block form: from Rr, Ri [mode][O][C]
+ * (float) build rbig [mode][2O][2C] = [[Rr,-Ri],[Ri,Rr]] in bfloat16, and fold
+ * a gradient of that block form back to dRr = d00 + d11, dRi = d10 - d01. */
+int fno_rbig_build(const float *rr, const float *ri, void *rbig_bf16, long long nmodes, int O, int C, void *stream);
+int fno_rbig_fold(const float *drbig, float *drr, float *dri, long long nmodes, int O, int C, void *stream);
 
 #ifdef __cplusplus
 }

@@ -31,6 +31,17 @@ def test_header_symbols_exported():
     assert exported == set(declared)
 
 
+def test_fno_header_symbols_exported():
+    from fortress_b200 import fno
+    hdr = open(os.path.join(ROOT, "include", "fno.h")).read()
+    declared = set(re.findall(r"^int (fno_[a-z0-9_]+)\(", hdr, re.M))
+    assert declared == set(fno.FNO_EXPORTS)
+    out = subprocess.run(["nm", "-D", "--defined-only", _abi.LIB_PATH], capture_output=True, text=True).stdout
+    assert set(re.findall(r" T (fno_[a-z0-9_]+)", out)) == declared
+    L = fno.lib()                      # argtypes bind without a device
+    assert L.fno_gemm.restype is not None
+
+
 def test_params_layout_matches_c(tmp_path):
     src = tmp_path / "layout.c"
     src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "fgpe.h"\n'
