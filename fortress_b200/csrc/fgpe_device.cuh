@@ -234,6 +234,7 @@ struct StepConst {
     const double *vx, *vy, *vz;     // ALPHA^2 X^2 etc. (V is their sum)
     const void *twx, *twy, *twz;    // twiddle tables, complex T
     const void *kex, *key, *kez;    // kinetic factors: kex[nx], key[ny], kez[ms*nz]
+    const void *pvx, *pvy, *pvz;    // potential factors exp(-i CDT ALPHA^2 X^2) per axis
     const int *fx, *fy, *fz;        // spectral position -> frequency index
     FftPlan px, py, pz;
 };
@@ -418,10 +419,12 @@ __device__ __forceinline__ void se_spin2(const StepConst& c, cx<T>* v) {
     // Number of Taylor terms fixed beforehand: the remainder after K terms is
     // below hn^(K+1)/(K+1)! * e^hn relative to |v|, and |y| >= e^-hn |v|
     // (e^{-h H} can contract by at most e^-hn), so stop once
-    // hn^(K+1)/(K+1)! * e^(2 hn) <= eps.  hn <= 1/2 keeps K <= 18 in FP64.
+    // hn^(K+1)/(K+1)! * e^(2 hn) <= eps.  On 0 <= hn <= 1/2, e^(2 hn) lies
+    // below its chord 1 + 2 (e - 1) hn < 1 + 4 hn, which stands in for it.
+    // hn <= 1/2 keeps K <= 18 in FP64.
     int K = 1;
     {
-        const T e2 = exp_t((T)2 * hn);
+        const T e2 = (T)1 + (T)4 * hn;
         T bnd = hn * hn * (T)0.5;
         while (bnd * e2 > Eps<T>::v() * (T)0.5 && K < 40) { ++K; bnd *= hn / (T)(K + 1); }
     }
@@ -498,12 +501,22 @@ template <typename T> __device__ __forceinline__ cx<T> small_phase(int imag, T t
     return mk<T>(cs, -sn);
 }
 
+// exp(-i CDT V) at grid point (i, j, k): V = vx + vy + vz is separable, so
+// the factor is the product of the per-axis tables.
+template <typename T>
+__device__ __forceinline__ cx<T> pot_phase(const StepConst& c, int i, int j, int k) {
+    cx<T> e = ((const cx<T>*)c.pvx)[i];
+    if (c.dim >= 2) e = cmul(e, ((const cx<T>*)c.pvy)[j]);
+    if (c.dim >= 3) e = cmul(e, ((const cx<T>*)c.pvz)[k]);
+    return e;
+}
+
 // SP (cgpe1d.f90:847-896): phi_m <- phi_m exp(-i CDT T_m), densities after SE.
-// T_m = A + B_m with the common part A = V + tau0 rho; exp(-i CDT A) is
-// computed once and the component parts B_m (tau1/tau2 terms, small for
-// physical states) by small_phase when |dt B_m| <= 1/16.
+// T_m = V + tau0 rho + B_m.  exp(-i CDT V) = eV comes from the per-axis
+// tables (pot_phase); the density parts tau0 rho and B_m (tau1/tau2 terms)
+// are small for physical states and use small_phase when |dt x| <= 1/16.
 template <typename T, int MS>
-__device__ __forceinline__ void apply_sp(const StepConst& c, T V, cx<T>* v) {
+__device__ __forceinline__ void apply_sp(const StepConst& c, cx<T> eV, cx<T>* v) {
     const T t0 = (T)c.tau0, t1 = (T)c.tau1, t2 = (T)c.tau2;
     T a[MS], rho = 0;
 #pragma unroll
@@ -522,7 +535,8 @@ __device__ __forceinline__ void apply_sp(const StepConst& c, T V, cx<T>* v) {
         B[MS - 1] = (T)-2 * t1 * fz + (T)0.4 * t2 * a[0];
     }
     const T dt = (T)c.dt;
-    const cx<T> eA = cdt_phase<T>(c.imag, dt, V + t0 * rho);
+    const T th0 = dt * t0 * rho;
+    const cx<T> eA = cmul(eV, fabs(th0) <= (T)0.0625 ? small_phase<T>(c.imag, th0) : cdt_phase<T>(c.imag, dt, t0 * rho));
 #pragma unroll
     for (int m = 0; m < MS; ++m) {
         const T th = dt * B[m];

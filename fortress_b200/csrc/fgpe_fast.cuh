@@ -229,11 +229,9 @@ __global__ void __launch_bounds__(TH, FGPE_ROW_MINB) k_row_fast(StepConst c, Row
                 cx<T> v[MS];
 #pragma unroll
                 for (int m = 0; m < MS; ++m) v[m] = cur[(m * R + r) * LP + x + (x >> 3)];
-                double V = c.vx[x];
-                if (c.dim >= 2) V += c.vy[j];
-                if (c.dim >= 3) V += c.vz[k];
+                const cx<T> eV = pot_phase<T>(c, x, j, k);
                 apply_se<T, MS>(c, v);
-                apply_sp<T, MS>(c, (T)V, v);
+                apply_sp<T, MS>(c, eV, v);
                 double w = c.wx[x];
                 if (c.dim >= 2) w *= c.wy[j];
                 if (c.dim >= 3) w *= c.wz[k];

@@ -131,11 +131,9 @@ k_row(StepConst c, RowArgs a) {
             cx<T> v[MS];
 #pragma unroll
             for (int m = 0; m < MS; ++m) v[m] = sm[(m * R + r) * lp + pad_idx(x)];
-            double V = c.vx[x];
-            if (c.dim >= 2) V += c.vy[j];
-            if (c.dim >= 3) V += c.vz[k];
+            const cx<T> eV = pot_phase<T>(c, x, j, k);
             apply_se<T, MS>(c, v);
-            apply_sp<T, MS>(c, (T)V, v);
+            apply_sp<T, MS>(c, eV, v);
             double w = c.wx[x];
             if (c.dim >= 2) w *= c.wy[j];
             if (c.dim >= 3) w *= c.wz[k];
@@ -260,7 +258,7 @@ k_1d(StepConst c, OneDArgs a) {
 #pragma unroll
             for (int m = 0; m < MS; ++m) v[m] = cscale(sm[m * lp + pad_idx(x)], invn);
             apply_se<T, MS>(c, v);
-            apply_sp<T, MS>(c, (T)c.vx[x], v);
+            apply_sp<T, MS>(c, pot_phase<T>(c, x, 0, 0), v);
             const double w = c.wx[x];
 #pragma unroll
             for (int m = 0; m < MS; ++m) {
@@ -558,12 +556,7 @@ __global__ void k_pointwise_op(StepConst c, PointArgs a) {
             case OP_KE: apply_ke<T, MS>(c, i, j, k, v); break;
             case OP_SOC: apply_soc<T, MS>(c, c.kx[i], c.dim >= 2 ? c.ky[j] : 0.0, v); break;
             case OP_SE: apply_se<T, MS>(c, v); break;
-            case OP_SP: {
-                double V = c.vx[i];
-                if (c.dim >= 2) V += c.vy[j];
-                if (c.dim >= 3) V += c.vz[k];
-                apply_sp<T, MS>(c, (T)V, v);
-            } break;
+            case OP_SP: apply_sp<T, MS>(c, pot_phase<T>(c, i, j, k), v); break;
             case OP_SCALE: {
 #pragma unroll
                 for (int m = 0; m < MS; ++m) v[m] = cscale(v[m], (T)a.factor);
