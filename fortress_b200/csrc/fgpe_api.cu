@@ -167,8 +167,20 @@ constexpr int fast_threads(int tot) {
     const int per = (tot + iter - 1) / iter;
     return (per + 31) / 32 * 32;
 }
-template <typename T, int MS, int N> constexpr int row_th() { return fast_threads(MS * row_r(N) * N / 8); }
-template <typename T, int MS, int N> constexpr int col_th() { return fast_threads(MS * col_tx<T>() * N / 8); }
+// Thread counts of the size-specialised kernels: one radix-8 butterfly per
+// thread and pass unless FGPE_ROW_TH / FGPE_COL_TH fix them at build time.
+#ifndef FGPE_ROW_TH
+#define FGPE_ROW_TH 0
+#endif
+#ifndef FGPE_COL_TH
+#define FGPE_COL_TH 0
+#endif
+template <typename T, int MS, int N> constexpr int row_th() {
+    return FGPE_ROW_TH ? FGPE_ROW_TH : fast_threads(MS * row_r(N) * N / 8);
+}
+template <typename T, int MS, int N> constexpr int col_th() {
+    return FGPE_COL_TH ? FGPE_COL_TH : fast_threads(MS * col_tx<T>() * N / 8);
+}
 template <typename T, int MS, int N> constexpr size_t row_smem() {
     return ((size_t)FGPE_ROW_NBUF * MS * row_r(N) * cpad(N) + (FGPE_TW_SMEM ? N : 0)) * sizeof(cx<T>);
 }
@@ -481,7 +493,7 @@ int fgpe_create(const fgpe_params* pin, fgpe_t** out) {
     }
     // complex tables (as doubles; converted to T below)
     std::vector<double> ct;
-    size_t off_tw[3], off_ke[3];
+    size_t off_tw[3], off_ke[3], off_pv[3];
     auto phase = [&](double xx, double* re, double* im) {  // exp(-i CDT xx)
         if (p.imag_time) { *re = exp(-p.dt * xx); *im = 0.0; }
         else { *re = cos(p.dt * xx); *im = -sin(p.dt * xx); }
@@ -514,6 +526,17 @@ int fgpe_create(const fgpe_params* pin, fgpe_t** out) {
                     ct.push_back(re); ct.push_back(im);
                 }
             }
+        }
+    }
+
+    for (int a = 0; a < 3; ++a) {
+        // exp(-i CDT ALPHA^2 X^2) per axis (1 on unused axes)
+        const double* v = &dt_all[off_v[a]];
+        off_pv[a] = ct.size() / 2;
+        for (int i = 0; i < ns[a]; ++i) {
+            double re, im;
+            phase(a < p.dim ? v[i] : 0.0, &re, &im);
+            ct.push_back(re); ct.push_back(im);
         }
     }
 
@@ -553,6 +576,7 @@ int fgpe_create(const fgpe_params* pin, fgpe_t** out) {
     c.vx = h->dtab + off_v[0]; c.vy = h->dtab + off_v[1]; c.vz = h->dtab + off_v[2];
     c.twx = (char*)h->ctab + off_tw[0] * ces; c.twy = (char*)h->ctab + off_tw[1] * ces; c.twz = (char*)h->ctab + off_tw[2] * ces;
     c.kex = (char*)h->ctab + off_ke[0] * ces; c.key = (char*)h->ctab + off_ke[1] * ces; c.kez = (char*)h->ctab + off_ke[2] * ces;
+    c.pvx = (char*)h->ctab + off_pv[0] * ces; c.pvy = (char*)h->ctab + off_pv[1] * ces; c.pvz = (char*)h->ctab + off_pv[2] * ces;
 
     // ---- launch shapes
     const size_t budget = 100 * 1024;   // two blocks per SM
