@@ -38,6 +38,7 @@ EXPORTS = (
     "fgpe_batch_create", "fgpe_batch_destroy", "fgpe_batch_size", "fgpe_batch_instance",
     "fgpe_batch_last_error", "fgpe_batch_config", "fgpe_batch_step", "fgpe_batch_observables",
     "fgpe_batch_autotune", "fgpe_batch_tuning", "fgpe_set_kernels", "fgpe_normc_noalloc",
+    "fgpe_checkpoint_save", "fgpe_checkpoint_load",
 )
 
 
@@ -105,6 +106,8 @@ def load():
         "fgpe_set_kernels": ([vp, ip], ip),
         "fgpe_normc_noalloc": ([ip, ip, ip, ip, ip, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                 vp, vp, vp], ip),
+        "fgpe_checkpoint_save": ([vp, ctypes.c_char_p, ctypes.c_longlong, dp], ip),
+        "fgpe_checkpoint_load": ([vp, ctypes.c_char_p, ctypes.POINTER(ctypes.c_longlong), dp], ip),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

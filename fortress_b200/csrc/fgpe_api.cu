@@ -1423,6 +1423,113 @@ int fno_rbig_fold(const float* drbig, float* drr, float* dri, long long nmodes, 
 
 }  // extern "C"
 
+// ================================================================ checkpoints
+// Full-precision checkpoint of a handle's state, bit-exact on resume: the
+// raw device buffers that hold the state (real-space psi and/or the
+// x-spectral S, whichever are current) with the per-component pending scales,
+// the last NORMC and the projection's Newton start values (info[]).  The
+// reference has no checkpoint; a long imaginary-time run can stop at an STP
+// boundary and continue in another process.
+//
+// File layout (native byte order): "FGPECKP1", u32 version = 1, the
+// fgpe_params of the handle, i64 step, 8 caller doubles, u32 flags
+// (1 psi, 2 S, 4 norms), info[INFO_LEN], then psi and/or S (npts*M complex
+// of the handle's precision), then u64 FNV-1a of everything before it.
+namespace {
+const char kCkpMagic[8] = {'F', 'G', 'P', 'E', 'C', 'K', 'P', '1'};
+
+struct Fnv {
+    unsigned long long h = 1469598103934665603ULL;
+    void add(const void* p, size_t n) {
+        const unsigned char* b = (const unsigned char*)p;
+        for (size_t i = 0; i < n; ++i) { h ^= b[i]; h *= 1099511628211ULL; }
+    }
+};
+}  // namespace
+
+extern "C" int fgpe_checkpoint_save(fgpe_t* h, const char* path, long long step, const double* user) {
+    if (!h || !path) return fail(h, FGPE_E_ARG, "null argument");
+    if (!h->has_state) return fail(h, FGPE_E_STATE, "no state set");
+    const size_t bytes = (size_t)h->npts * h->ms * h->cs;
+    std::vector<unsigned char> psi, S;
+    if (h->psi_valid) { psi.resize(bytes); CK(cudaMemcpyAsync(psi.data(), h->psi, bytes, cudaMemcpyDeviceToHost, h->st)); }
+    if (h->S_valid) { S.resize(bytes); CK(cudaMemcpyAsync(S.data(), h->S, bytes, cudaMemcpyDeviceToHost, h->st)); }
+    double info[INFO_LEN];
+    CK(cudaMemcpyAsync(info, h->info, sizeof(info), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    const unsigned version = 1;
+    const unsigned flags = (h->psi_valid ? 1u : 0u) | (h->S_valid ? 2u : 0u) | (h->norms_valid ? 4u : 0u);
+    double u[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    if (user) memcpy(u, user, sizeof(u));
+    const std::string tmp = std::string(path) + ".tmp";
+    FILE* f = fopen(tmp.c_str(), "wb");
+    if (!f) return fail(h, FGPE_E_ARG, std::string("cannot open ") + tmp + " for writing");
+    Fnv fnv;
+    bool ok = true;
+    auto put = [&](const void* p, size_t n) {
+        if (!n) return;
+        fnv.add(p, n);
+        ok = ok && fwrite(p, 1, n, f) == n;
+    };
+    put(kCkpMagic, 8); put(&version, 4); put(&h->p, sizeof(fgpe_params)); put(&step, 8); put(u, sizeof(u));
+    put(&flags, 4); put(info, sizeof(info)); put(psi.data(), psi.size()); put(S.data(), S.size());
+    ok = ok && fwrite(&fnv.h, 1, 8, f) == 8;
+    ok = (fclose(f) == 0) && ok;
+    if (!ok || rename(tmp.c_str(), path) != 0) { remove(tmp.c_str()); return fail(h, FGPE_E_ARG, std::string("cannot write ") + path); }
+    return FGPE_OK;
+}
+
+extern "C" int fgpe_checkpoint_load(fgpe_t* h, const char* path, long long* step, double* user) {
+    if (!h || !path) return fail(h, FGPE_E_ARG, "null argument");
+    FILE* f = fopen(path, "rb");
+    if (!f) return fail(h, FGPE_E_ARG, std::string("cannot open ") + path);
+    std::vector<unsigned char> all;
+    {
+        unsigned char buf[1 << 16];
+        size_t n;
+        while ((n = fread(buf, 1, sizeof(buf), f)) > 0) all.insert(all.end(), buf, buf + n);
+        fclose(f);
+    }
+    const size_t bytes = (size_t)h->npts * h->ms * h->cs;
+    const size_t head = 8 + 4 + sizeof(fgpe_params) + 8 + 64 + 4 + sizeof(double) * INFO_LEN;
+    if (all.size() < head + 8 || memcmp(all.data(), kCkpMagic, 8) != 0)
+        return fail(h, FGPE_E_ARG, std::string(path) + " is not a checkpoint");
+    Fnv fnv;
+    fnv.add(all.data(), all.size() - 8);
+    unsigned long long sum;
+    memcpy(&sum, all.data() + all.size() - 8, 8);
+    if (sum != fnv.h) return fail(h, FGPE_E_ARG, std::string(path) + ": checksum mismatch");
+    size_t o = 8;
+    unsigned version, flags;
+    fgpe_params p;
+    long long st;
+    double u[8], info[INFO_LEN];
+    memcpy(&version, &all[o], 4); o += 4;
+    memcpy(&p, &all[o], sizeof(p)); o += sizeof(p);
+    memcpy(&st, &all[o], 8); o += 8;
+    memcpy(u, &all[o], 64); o += 64;
+    memcpy(&flags, &all[o], 4); o += 4;
+    memcpy(info, &all[o], sizeof(info)); o += sizeof(info);
+    if (version != 1) return fail(h, FGPE_E_ARG, "unsupported checkpoint version");
+    if (p.dim != h->p.dim || p.spin != h->p.spin || p.nx != h->p.nx || p.ny != h->p.ny || p.nz != h->p.nz ||
+        p.precision != h->p.precision)
+        return fail(h, FGPE_E_ARG, "checkpoint grid, spin or precision differs from the handle's");
+    const size_t want = head + ((flags & 1) ? bytes : 0) + ((flags & 2) ? bytes : 0) + 8;
+    if (all.size() != want || !(flags & 3)) return fail(h, FGPE_E_ARG, std::string(path) + ": truncated or malformed");
+    if (flags & 1) { CK(cudaMemcpyAsync(h->psi, &all[o], bytes, cudaMemcpyHostToDevice, h->st)); o += bytes; }
+    if (flags & 2) { CK(cudaMemcpyAsync(h->S, &all[o], bytes, cudaMemcpyHostToDevice, h->st)); o += bytes; }
+    CK(cudaMemcpyAsync(h->info, info, sizeof(info), cudaMemcpyHostToDevice, h->st));
+    CK(cudaStreamSynchronize(h->st));   // host buffers go out of scope
+    h->psi_valid = (flags & 1) != 0;
+    h->S_valid = (flags & 2) != 0;
+    h->norms_valid = (flags & 4) != 0;
+    h->prev_valid = false;
+    h->has_state = true;
+    if (step) *step = st;
+    if (user) memcpy(user, u, sizeof(u));
+    return FGPE_OK;
+}
+
 // ===================================================== NORMC without allocation
 // fgpe_normc_noalloc: NORMC of a caller's device-resident spinor with no
 // handle and no allocation of any kind.  Its only scratch is the file-scope

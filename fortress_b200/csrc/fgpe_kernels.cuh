@@ -52,8 +52,11 @@ __device__ __forceinline__ double block_max(double v, double* red) {
     return r;
 }
 
-// Last-block completion of the NORMC reduction: partial[b*MS+m] from every
-// block are summed in block order; info[] receives scale, total and norms.
+// Last-block completion of the NORMC reduction: the partials
+// partial[b*MS+m] of every block are summed by the whole last block in a
+// fixed order (thread t takes blocks t, t+T, ..., then the block tree), so
+// the result does not depend on which block finishes last; info[] receives
+// scale, total and norms.  red holds at least 32*(MS+1) doubles.
 template <int MS>
 __device__ __forceinline__ void finish_norms(const StepConst& c, const double* part, unsigned* counter,
                                              double* info, double* red) {
@@ -62,12 +65,17 @@ __device__ __forceinline__ void finish_norms(const StepConst& c, const double* p
     if (threadIdx.x == 0) is_last = (atomicAdd(counter, 1u) == gridDim.x * gridDim.y - 1);
     __syncthreads();
     if (!is_last) return;
+    __threadfence();
     const int nb = gridDim.x * gridDim.y;
-    if (threadIdx.x < MS) {
-        double s = 0;
-        for (int b = 0; b < nb; ++b) s += __ldcg(part + (size_t)b * MS + threadIdx.x);
-        red[threadIdx.x] = s;
+    double acc[MS];
+#pragma unroll
+    for (int m = 0; m < MS; ++m) acc[m] = 0.0;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+#pragma unroll
+        for (int m = 0; m < MS; ++m) acc[m] += __ldcg(part + (size_t)b * MS + m);
     }
+    block_sum<MS>(acc, red, red + 32 * MS);
+    if (threadIdx.x < MS) red[threadIdx.x] = red[32 * MS + threadIdx.x];
     __syncthreads();
     if (threadIdx.x == 0) {
         double tot = 0, n[MS], sc[MS];
@@ -503,14 +511,25 @@ k_obs(StepConst c, ObsArgs a) {
     if (threadIdx.x == 0) is_last = (atomicAdd(a.counter, 1u) == gridDim.x - 1);
     __syncthreads();
     if (!is_last) return;
+    // the whole last block adds the block partials in a fixed order (thread t
+    // takes blocks t, t+256, ..., then the block tree) and takes their max
+    __threadfence();
     const int nb = gridDim.x;
-    if (threadIdx.x <= NQ) {
-        double r = 0;
-        for (int b = 0; b < nb; ++b) {
-            const double v = __ldcg(a.part + (size_t)b * (NQ + 1) + threadIdx.x);
-            r = threadIdx.x == NQ ? fmax(r, v) : r + v;
-        }
-        red[threadIdx.x] = r;
+    double r[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) r[q] = 0.0;
+    double mx = 0.0;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+        const double* pb = a.part + (size_t)b * (NQ + 1);
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) r[q] += __ldcg(pb + q);
+        mx = fmax(mx, __ldcg(pb + NQ));
+    }
+    block_sum<NQ>(r, red, bsum);
+    const double gmax = block_max(mx, red);
+    if (threadIdx.x == 0) {
+        for (int q = 0; q < NQ; ++q) red[q] = bsum[q];
+        red[NQ] = gmax;
     }
     __syncthreads();
     if (threadIdx.x == 0) {

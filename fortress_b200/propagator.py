@@ -189,6 +189,20 @@ class Propagator:
     def set_kernels(self, kernels):
         self._ck(self._L.fgpe_set_kernels(self._h, {"auto": 0, "generic": 1, "fast-row": 2, "fast-col": 3}[kernels]))
 
+    def save(self, path, step=0, user=None):
+        """Full-precision checkpoint (fgpe_checkpoint_save); user: up to 8 floats."""
+        u = np.zeros(8)
+        if user is not None:
+            u[:len(user)] = user
+        self._ck(self._L.fgpe_checkpoint_save(self._h, str(path).encode(), int(step), _dp(u)))
+
+    def load(self, path):
+        """Restore a checkpoint; returns (step, user[8])."""
+        st = ctypes.c_longlong()
+        u = np.zeros(8)
+        self._ck(self._L.fgpe_checkpoint_load(self._h, str(path).encode(), ctypes.byref(st), _dp(u)))
+        return int(st.value), u
+
     def kernel_launches(self):
         c = ctypes.c_longlong()
         self._ck(self._L.fgpe_kernel_launches(self._h, ctypes.byref(c)))

@@ -176,6 +176,16 @@ int fgpe_batch_tuning(const fgpe_batch_t *b, int *width, int *steps_per_graph);
  * (same data layout, so this can happen between any two calls). */
 int fgpe_set_kernels(fgpe_t *h, int kernels);
 
+/* Full-precision checkpoint of the handle's state (no reference
+ * counterpart: FORTRESS restarts only from the F18.10 text of initial_sol).
+ * The raw device buffers, pending scales, last NORMC and the projection's
+ * Newton start values are written, so fgpe_checkpoint_load into a handle of
+ * the same grid, spin and precision continues bit-identically.  step and
+ * user[8] (may be NULL) are stored for the caller (e.g. II and EN_OLD).
+ * The file is written to path.tmp and renamed; a checksum guards loading. */
+int fgpe_checkpoint_save(fgpe_t *h, const char *path, long long step, const double *user);
+int fgpe_checkpoint_load(fgpe_t *h, const char *path, long long *step, double *user);
+
 /* NORMC of a spinor the caller already holds on the device, with no handle
  * and no allocation of any kind: for callers that may not allocate device
  * memory, such as a host code whose device memory is reserved up front by
