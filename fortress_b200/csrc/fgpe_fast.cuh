@@ -36,25 +36,39 @@ constexpr int cplan_block(int n, int pass) {
 constexpr int cpad(int n) { return n + (n + 7) / 8; }
 
 // ------------------------------------------------------------ line maps
+// A line map also names the groups of tasks that touch disjoint sets of
+// lines: GROUP(nb) consecutive tasks form one group when a pass has nb
+// butterflies per line.  With one task per thread, each group is a
+// contiguous run of threads that only reads and writes its own lines.
 template <int N, int NL> struct RowTile {
     static constexpr int LP = cpad(N);
     static __device__ __forceinline__ void split(int b, int nb, int& l, int& q) { l = b / nb; q = b - l * nb; }
     static __device__ __forceinline__ int at(int l, int e) { return l * LP + e + (e >> 3); }
+    static constexpr int GROUP(int nb) { return nb; }
 };
 template <int N, int TX> struct ColTile {
     static constexpr int LPN = cpad(N);
+    static constexpr int GROUP(int nb) { return nb * TX; }
     static __device__ __forceinline__ void split(int b, int nb, int& l, int& q) {
         const int t = b % TX; const int w = b / TX; q = w % nb; const int m = w / nb; l = m * TX + t;
     }
     static __device__ __forceinline__ int at(int l, int e) { return ((l / TX) * LPN + e + (e >> 3)) * TX + (l % TX); }
 };
 
-template <typename T, bool INV, int N, int NL, int TH, int P, class Map>
+// One radix-R pass over NL lines.  Between two passes only the threads that
+// share lines need to wait for each other: when every thread has exactly one
+// task in this pass and in the next (same radix, so the same task -> line
+// assignment) and the task groups are whole warps, the pass ends on the named
+// barrier of its group (ids 1..15) instead of the block barrier.  NEXT_R is
+// the radix of the next pass of the same transform, 0 after the last.
+template <typename T, bool INV, int N, int NL, int TH, int P, class Map, int NEXT_R = 0>
 __device__ __forceinline__ void ct_pass(cx<T>* s, const cx<T>* __restrict__ tw) {
     constexpr CPlan pl = cplan(N);
     constexpr int R = pl.r[P];
     constexpr int BP = cplan_block(N, P);
     constexpr int SI = BP / R, NB = N / R, TOT = NL * NB, ITER = (TOT + TH - 1) / TH, TSTEP = N / BP;
+    constexpr int GT = Map::GROUP(NB);
+    constexpr bool GROUPED = NEXT_R == R && TOT == TH && GT % 32 == 0 && TOT % GT == 0 && TOT / GT <= 15;
 #pragma unroll
     for (int it = 0; it < ITER; ++it) {
         const int b = threadIdx.x + it * TH;
@@ -82,7 +96,12 @@ __device__ __forceinline__ void ct_pass(cx<T>* s, const cx<T>* __restrict__ tw) 
             for (int r = 0; r < R; ++r) s[Map::at(l, e0 + r * SI)] = v[r];
         }
     }
-    __syncthreads();
+    if constexpr (GROUPED) {
+        const int g = (int)threadIdx.x / GT;
+        asm volatile("bar.sync %0, %1;\n" ::"r"(1 + g), "r"(GT) : "memory");
+    } else {
+        __syncthreads();
+    }
 }
 
 template <typename T, bool INV, int N, int NL, int TH, class Map, int P = 0>
@@ -90,7 +109,8 @@ __device__ __forceinline__ void ct_fft(cx<T>* s, const cx<T>* __restrict__ tw) {
     constexpr CPlan pl = cplan(N);
     if constexpr (P < pl.nf) {
         constexpr int PP = INV ? pl.nf - 1 - P : P;
-        ct_pass<T, INV, N, NL, TH, PP, Map>(s, tw);
+        constexpr int NEXT_R = P + 1 < pl.nf ? pl.r[INV ? PP - 1 : PP + 1] : 0;
+        ct_pass<T, INV, N, NL, TH, PP, Map, NEXT_R>(s, tw);
         ct_fft<T, INV, N, NL, TH, Map, P + 1>(s, tw);
     }
 }
@@ -324,7 +344,10 @@ __global__ void __launch_bounds__(TH, FGPE_COL_MINB) k_col_fast(StepConst c, Col
         const int x0 = (tile % nxt) * TX;
         const int oth = tile / nxt;
         const long long off = (long long)oth * a.other_stride + x0;
-        if (a.flags & COL_SCALE) {
+        // with KE/SOC in this pass the scale rides on the pointwise step
+        // (the transform is linear); otherwise it takes its own sweep
+        const bool fold = (a.flags & COL_SCALE) && (a.flags & COL_KOP);
+        if ((a.flags & COL_SCALE) && !fold) {
             for (int idx = threadIdx.x; idx < MS * N * TX; idx += TH) {
                 const int t = idx % TX, q = idx / TX, e = q % N, m = q / N;
                 cx<T>& v = cur[(m * LPN + e + (e >> 3)) * TX + t];
@@ -342,6 +365,10 @@ __global__ void __launch_bounds__(TH, FGPE_COL_MINB) k_col_fast(StepConst c, Col
                 cx<T> v[MS];
 #pragma unroll
                 for (int m = 0; m < MS; ++m) v[m] = cur[(m * LPN + e + (e >> 3)) * TX + t];
+                if (fold) {
+#pragma unroll
+                    for (int m = 0; m < MS; ++m) v[m] = cscale(v[m], fac[m]);
+                }
                 apply_ke<T, MS>(c, ix, iy, iz, v);
                 apply_soc<T, MS>(c, c.kx[ix], c.dim >= 2 ? c.ky[iy] : 0.0, v);
 #pragma unroll
