@@ -208,11 +208,38 @@ template <typename T, int MS, int N> int setup_fast_col(fgpe_t* h, int ntiles) {
     return grid_for(k_col_fast<T, MS, N, col_tx<T>(), col_th<T, MS, N>()>, col_th<T, MS, N>(), col_smem<T, MS, N>(),
                     ntiles);
 }
+// The size-specialised kernels go out as programmatic dependent launches
+// (outside stream capture): the next pass is launched while the previous one
+// drains and waits on griddepcontrol.wait before it touches the state.  Their
+// grids are one wave of resident blocks, so a waiting block never keeps the
+// previous pass from finishing.
+template <class K, class A>
+void launch_pdl(fgpe_t* h, K kern, int grid, int threads, size_t smem, const A& a) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(h->st, &cs);
+    if (cs != cudaStreamCaptureStatusNone) {
+        kern<<<grid, threads, smem, h->st>>>(h->sc, a);
+        return;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(threads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = h->st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kern, h->sc, a);
+}
 template <typename T, int MS, int N> void run_fast_row(fgpe_t* h, const RowArgs& a) {
-    k_row_fast<T, MS, N, row_r(N), row_th<T, MS, N>()><<<h->fast_row_grid, row_th<T, MS, N>(), row_smem<T, MS, N>(), h->st>>>(h->sc, a);
+    launch_pdl(h, k_row_fast<T, MS, N, row_r(N), row_th<T, MS, N>()>, h->fast_row_grid, row_th<T, MS, N>(),
+               row_smem<T, MS, N>(), a);
 }
 template <typename T, int MS, int N> void run_fast_col(fgpe_t* h, int axis, const ColArgs& a) {
-    k_col_fast<T, MS, N, col_tx<T>(), col_th<T, MS, N>()><<<h->fast_col_grid[axis], col_th<T, MS, N>(), col_smem<T, MS, N>(), h->st>>>(h->sc, a);
+    launch_pdl(h, k_col_fast<T, MS, N, col_tx<T>(), col_th<T, MS, N>()>, h->fast_col_grid[axis], col_th<T, MS, N>(),
+               col_smem<T, MS, N>(), a);
 }
 
 #define FAST_SWITCH(n, CALL)            \

@@ -175,6 +175,9 @@ template <int N> __device__ __forceinline__ void cp_wait() { asm volatile("cp.as
 // Tiles of R x-lines (all MS components); see k_row for the three modes.
 template <typename T, int MS, int N, int R, int TH, int NBUF = FGPE_ROW_NBUF>
 __global__ void __launch_bounds__(TH, FGPE_ROW_MINB) k_row_fast(StepConst c, RowArgs a) {
+    // a programmatic dependent launch starts before the previous pass ends:
+    // wait for it (and its memory) before touching the state
+    asm volatile("griddepcontrol.wait;\n" ::: "memory");
     using RT = RowTile<N, MS * R>;
     constexpr int LP = RT::LP;
     constexpr int TILE = MS * R * LP;
@@ -275,6 +278,7 @@ __global__ void __launch_bounds__(TH, FGPE_ROW_MINB) k_row_fast(StepConst c, Row
         __syncthreads();
     }
     cp_wait<0>();
+    asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
     if (a.mode != ROW_FULL) return;
     block_sum<MS>(acc, red, bsum);
     if (threadIdx.x < MS) a.part[(size_t)blockIdx.x * MS + threadIdx.x] = bsum[threadIdx.x];
@@ -286,6 +290,7 @@ __global__ void __launch_bounds__(TH, FGPE_ROW_MINB) k_row_fast(StepConst c, Row
 // axis; persistent over (x-tile, other) pairs.
 template <typename T, int MS, int N, int TX, int TH, int NBUF = FGPE_COL_NBUF>
 __global__ void __launch_bounds__(TH, FGPE_COL_MINB) k_col_fast(StepConst c, ColArgs a) {
+    asm volatile("griddepcontrol.wait;\n" ::: "memory");
     using CT = ColTile<N, TX>;
     constexpr int LPN = CT::LPN;
     constexpr int TILE = MS * LPN * TX;
@@ -384,6 +389,7 @@ __global__ void __launch_bounds__(TH, FGPE_COL_MINB) k_col_fast(StepConst c, Col
         __syncthreads();
     }
     cp_wait<0>();
+    asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
 }
 
 }  // namespace fgpe
