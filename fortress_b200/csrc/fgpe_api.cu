@@ -59,6 +59,7 @@ struct fgpe_s {
     bool fast_row = false, fast_col[3] = {false, false, false};
     bool has_fast_row = false, has_fast_col[3] = {false, false, false};
     int fast_row_grid = 0, fast_col_grid[3] = {0, 0, 0};
+    bool col_wide[3] = {false, false, false};   // column pass uses the wide tiles
     bool psi_valid = false, S_valid = false, prev_valid = false, norms_valid = false, has_state = false;
     long long launches = 0;
     std::string msg;
@@ -181,6 +182,15 @@ template <typename T, int MS, int N> constexpr int row_th() {
 template <typename T, int MS, int N> constexpr int col_th() {
     return FGPE_COL_TH ? FGPE_COL_TH : fast_threads(MS * col_tx<T>() * N / 8);
 }
+// Wide column tiles: 128 contiguous bytes of x per line element (8 complex
+// doubles, 16 complex floats), for grids with enough tiles (3D) where the
+// 32-byte segments of the narrow tiles waste DRAM bursts.
+template <typename T> constexpr int col_txw() { return 128 / (int)sizeof(cx<T>); }
+template <typename T, int MS, int N> constexpr size_t col_smem_w() {
+    return (size_t)FGPE_COL_NBUF * MS * cpad(N) * col_txw<T>() * sizeof(cx<T>);
+}
+template <typename T, int MS, int N> constexpr bool wide_ok() { return col_smem_w<T, MS, N>() <= 113 * 1024; }
+template <typename T, int MS, int N> constexpr int col_th_w() { return fast_threads(MS * col_txw<T>() * N / 8); }
 template <typename T, int MS, int N> constexpr size_t row_smem() {
     return ((size_t)FGPE_ROW_NBUF * MS * row_r(N) * cpad(N) + (FGPE_TW_SMEM ? N : 0)) * sizeof(cx<T>);
 }
@@ -203,10 +213,22 @@ template <typename T, int MS, int N> int setup_fast_row(fgpe_t* h) {
     return grid_for(k_row_fast<T, MS, N, row_r(N), row_th<T, MS, N>()>, row_th<T, MS, N>(), row_smem<T, MS, N>(),
                     rows / row_r(N));
 }
-template <typename T, int MS, int N> int setup_fast_col(fgpe_t* h, int ntiles) {
+// Grid of the column kernel for one axis (0: none); *wide tells whether the
+// wide tiles were chosen: they need 128-byte rows of x and at least four
+// waves of tiles, so that their fewer, larger tiles still fill the GPU.
+template <typename T, int MS, int N> int setup_fast_col(fgpe_t* h, int n_other, bool* wide) {
+    *wide = false;
+    if constexpr (wide_ok<T, MS, N>()) {
+        if (h->p.nx % col_txw<T>() == 0) {
+            const int ntw = (h->p.nx / col_txw<T>()) * n_other;
+            const int g = grid_for(k_col_fast<T, MS, N, col_txw<T>(), col_th_w<T, MS, N>()>, col_th_w<T, MS, N>(),
+                                   col_smem_w<T, MS, N>(), ntw);
+            if (g > 0 && ntw >= 4 * g) { *wide = true; return g; }
+        }
+    }
     if (h->p.nx % col_tx<T>()) return 0;
     return grid_for(k_col_fast<T, MS, N, col_tx<T>(), col_th<T, MS, N>()>, col_th<T, MS, N>(), col_smem<T, MS, N>(),
-                    ntiles);
+                    (h->p.nx / col_tx<T>()) * n_other);
 }
 // The size-specialised kernels go out as programmatic dependent launches
 // (outside stream capture): the next pass is launched while the previous one
@@ -238,6 +260,13 @@ template <typename T, int MS, int N> void run_fast_row(fgpe_t* h, const RowArgs&
                row_smem<T, MS, N>(), a);
 }
 template <typename T, int MS, int N> void run_fast_col(fgpe_t* h, int axis, const ColArgs& a) {
+    if constexpr (wide_ok<T, MS, N>()) {
+        if (h->col_wide[axis]) {
+            launch_pdl(h, k_col_fast<T, MS, N, col_txw<T>(), col_th_w<T, MS, N>()>, h->fast_col_grid[axis],
+                       col_th_w<T, MS, N>(), col_smem_w<T, MS, N>(), a);
+            return;
+        }
+    }
     launch_pdl(h, k_col_fast<T, MS, N, col_tx<T>(), col_th<T, MS, N>()>, h->fast_col_grid[axis], col_th<T, MS, N>(),
                col_smem<T, MS, N>(), a);
 }
@@ -668,13 +697,14 @@ int fgpe_create(const fgpe_params* pin, fgpe_t** out) {
     }
     for (int a = 1; a < p.dim; ++a) {
         if (!allow_fast_col || !fast_size(ns[a])) continue;
-        const int ntl = (p.nx / (h->fp32 ? col_tx<float>() : col_tx<double>())) * (p.dim == 2 ? 1 : (a == 1 ? p.nz : p.ny));
+        const int nob = p.dim == 2 ? 1 : (a == 1 ? p.nz : p.ny);
         int g = 0;
-#define SETC(NN) g = h->fp32 ? (ms == 3 ? setup_fast_col<float, 3, NN>(h, ntl) : setup_fast_col<float, 5, NN>(h, ntl)) \
-                             : (ms == 3 ? setup_fast_col<double, 3, NN>(h, ntl) : setup_fast_col<double, 5, NN>(h, ntl))
+        bool wide = false;
+#define SETC(NN) g = h->fp32 ? (ms == 3 ? setup_fast_col<float, 3, NN>(h, nob, &wide) : setup_fast_col<float, 5, NN>(h, nob, &wide)) \
+                             : (ms == 3 ? setup_fast_col<double, 3, NN>(h, nob, &wide) : setup_fast_col<double, 5, NN>(h, nob, &wide))
         FAST_SWITCH(ns[a], SETC)
 #undef SETC
-        if (g > 0) { h->fast_col[a] = h->has_fast_col[a] = true; h->fast_col_grid[a] = g; }
+        if (g > 0) { h->fast_col[a] = h->has_fast_col[a] = true; h->fast_col_grid[a] = g; h->col_wide[a] = wide; }
     }
     cudaGetLastError();   // clear any attribute/occupancy probe error
     h->obsl.grid = dim3((unsigned)((h->npts + 255) / 256));

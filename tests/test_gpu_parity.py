@@ -133,6 +133,31 @@ def test_fast_matches_generic_512(F, precision):
     assert rel_err(a.state(), b.state()) < tol
 
 
+WIDE_CASES = [((3, 1, 1, (128, 128, 128)), "fp64"), ((3, 2, 0, (128, 128, 128)), "fp64"),
+              ((3, 1, 0, (256, 128, 128)), "fp32")]
+
+
+@pytest.mark.parametrize("case,precision", WIDE_CASES, ids=lambda v: case_id(v) if isinstance(v, tuple) else v)
+def test_wide_column_tiles_match_generic(F, case, precision):
+    """3D grids with enough column tiles take the wide (128-byte) column
+    tiles; they agree with the generic kernels (GPU only, 6 steps)."""
+    p = case_params(case)
+    rng = np.random.default_rng(6)
+    axes = np.meshgrid(*[(np.arange(n) - n / 2) * d for n, d in zip(case[3], p["d"])], indexing="ij")
+    g = np.exp(-sum(a ** 2 for a in axes) / 8.0)
+    ms = 2 * case[1] + 1
+    phi = np.stack([g * np.exp(1j * rng.uniform(-0.3, 0.3, g.shape)) for _ in range(ms)], axis=-1)
+    a = F.Propagator(**p, precision=precision)
+    b = F.Propagator(**p, precision=precision, kernels="generic")
+    a.set_state(phi); b.set_state(phi)
+    if case[2]:
+        a.normt(); b.normt()
+    a.step(6); b.step(6)
+    tol = 1e-12 if precision == "fp64" else 1e-5
+    assert rel_err(a.state(), b.state()) < tol
+    assert np.allclose(a.normc(), b.normc(), rtol=tol)
+
+
 PROJ_CASES = [(1, 1, 1, (96,)), (1, 2, 1, (64,)), (2, 1, 1, (32, 24)), (2, 2, 1, (32, 32)),
               (3, 1, 1, (16, 16, 12)), (3, 2, 1, (16, 12, 16)), (2, 2, 1, (128, 192))]
 
