@@ -162,7 +162,12 @@ constexpr int kFastN[] = {128, 192, 256, 384, 512};
 #define FGPE_COL_TX32 2
 #endif
 template <typename T> constexpr int col_tx() { return sizeof(T) == 8 ? 2 : FGPE_COL_TX32; }
-constexpr int row_r(int n) { return n >= 384 ? 1 : 512 / n; }
+// Rows per row-kernel tile (FGPE_ROW_R256 fixes it for 256-point rows at
+// build time).
+#ifndef FGPE_ROW_R256
+#define FGPE_ROW_R256 0
+#endif
+constexpr int row_r(int n) { return n >= 384 ? 1 : (n == 256 && FGPE_ROW_R256 ? FGPE_ROW_R256 : 512 / n); }
 constexpr int fast_threads(int tot) {
     const int iter = (tot + 511) / 512;
     const int per = (tot + iter - 1) / iter;

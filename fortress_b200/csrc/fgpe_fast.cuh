@@ -155,9 +155,13 @@ template <int N> __device__ __forceinline__ void cp_wait() { asm volatile("cp.as
 
 // Blocks per SM the launch bounds target and shared buffers per block
 // (2 = double-buffered prefetch).
+// Resident blocks per SM the row kernel is compiled for: small blocks (up to
+// 192 threads: the spin-1 rows) run 4 per SM, the others 2, unless
+// FGPE_ROW_MINB fixes it at build time.
 #ifndef FGPE_ROW_MINB
-#define FGPE_ROW_MINB 2
+#define FGPE_ROW_MINB 0
 #endif
+constexpr int row_minb(int th) { return FGPE_ROW_MINB ? FGPE_ROW_MINB : (th <= 192 ? 4 : 2); }
 #ifndef FGPE_ROW_NBUF
 #define FGPE_ROW_NBUF 2
 #endif
@@ -174,7 +178,7 @@ template <int N> __device__ __forceinline__ void cp_wait() { asm volatile("cp.as
 // ------------------------------------------------------------ row kernel
 // Tiles of R x-lines (all MS components); see k_row for the three modes.
 template <typename T, int MS, int N, int R, int TH, int NBUF = FGPE_ROW_NBUF>
-__global__ void __launch_bounds__(TH, FGPE_ROW_MINB) k_row_fast(StepConst c, RowArgs a) {
+__global__ void __launch_bounds__(TH, row_minb(TH)) k_row_fast(StepConst c, RowArgs a) {
     // a programmatic dependent launch starts before the previous pass ends:
     // wait for it (and its memory) before touching the state
     asm volatile("griddepcontrol.wait;\n" ::: "memory");
