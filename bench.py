@@ -179,11 +179,29 @@ def run_cpu(phi, cfg, steps, warmup, budget_s=None):
 
 
 def capture(args):
-    """The headline step alone: warmup + steps split steps of the 512^2 spin-2
-    real-time case from the noisy Gaussian guess, for ncu launch lists and
-    per-kernel captures (-k regex:k_row_fast / k_col_fast)."""
+    """The step kernels alone, for ncu launch lists and per-kernel captures
+    (-k regex:k_row_fast / k_col_fast): warmup + steps split steps of the
+    512^2 spin-2 real-time case from the noisy Gaussian guess, or with
+    --workload 3d of the 3D spin-1 case on a 128^3 grid (the same kernel
+    families, wide column tiles included, at an eighth of the 256^3 state:
+    a small case for ncu)."""
     import numpy as np
     import fortress_b200 as F
+    if args.workload == "3d":
+        from fortress_b200.config import RunConfig
+        w = D3
+        cfg = RunConfig(dim=3, spin=1, n=(128, 128, 128), d=(0.2, 0.2, 0.2), dt=w["dt"], mass=w["mass"],
+                        a=w["a"], natoms=w["natoms"], nu=w["nu"], switch_im=1, gamma=w["gamma"])
+        p = cfg.params(args.precision)
+        prop = F.Propagator(**p)
+        prop.set_state(gaussian_nd(p))
+        prop.normt()
+        prop.step(args.warmup + args.steps, snapshot=False)
+        n = prop.normc()
+        assert np.all(np.isfinite(n))
+        print(json.dumps({"capture": "3d-spin1-SO-imag-128^3", "precision": args.precision,
+                          "steps": args.warmup + args.steps, "norm": float(n.sum())}))
+        return
     cfg = workload_config(WORKLOAD["gamma"])
     prop = F.Propagator(**cfg.params(args.precision))
     prop.set_state(add_noise(gaussian_guess(cfg)))
@@ -491,9 +509,9 @@ def other_workload(args):
     npts = sum(int(np.prod(p["n"])) for p in insts)
     b.step(max(args.warmup, 4))
     clocks.start()
-    t0 = time.perf_counter()
-    b.step(args.steps)
-    el = time.perf_counter() - t0
+    steps = args.steps + (1 if args.steps % tune[1] == 1 else 0)   # whole graph launches only
+    el = b.step_timed(steps) / 1e3                                # CUDA events on the launch stream
+    args.steps = steps
     clk = clocks.stop()
     cs = 16 if args.precision == "fp64" else 8
     res = {"metric": METRIC, "value": npts * args.steps / el, "unit": "grid-pt*steps/s", "n_gpus": 1,
