@@ -38,7 +38,7 @@ EXPORTS = (
     "fgpe_batch_create", "fgpe_batch_destroy", "fgpe_batch_size", "fgpe_batch_instance",
     "fgpe_batch_last_error", "fgpe_batch_config", "fgpe_batch_step", "fgpe_batch_observables",
     "fgpe_batch_autotune", "fgpe_batch_tuning", "fgpe_set_kernels", "fgpe_normc_noalloc",
-    "fgpe_checkpoint_save", "fgpe_checkpoint_load",
+    "fgpe_checkpoint_save", "fgpe_checkpoint_load", "fgpe_batch_step_timed",
 )
 
 
@@ -100,6 +100,7 @@ def load():
         "fgpe_batch_last_error": ([vp], ctypes.c_char_p),
         "fgpe_batch_config": ([vp, ip, ip], ip),
         "fgpe_batch_step": ([vp, ip], ip),
+        "fgpe_batch_step_timed": ([vp, ip, dp], ip),
         "fgpe_batch_observables": ([vp, dp, ip], ip),
         "fgpe_batch_autotune": ([vp, ip, ctypes.c_char_p], ip),
         "fgpe_batch_tuning": ([vp, ctypes.POINTER(ip), ctypes.POINTER(ip)], ip),

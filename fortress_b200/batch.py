@@ -67,6 +67,12 @@ class Batch:
     def step(self, n):
         check_batch(self._L.fgpe_batch_step(self._b, int(n)), self._b)
 
+    def step_timed(self, n):
+        """n steps as whole graph launches; returns their device time in ms."""
+        ms = ctypes.c_double()
+        check_batch(self._L.fgpe_batch_step_timed(self._b, int(n), ctypes.byref(ms)), self._b)
+        return ms.value
+
     def observables(self, with_conv=True):
         """Per instance: dict(en, mz, conv, mu, rms, norm)."""
         ms = [p.ms for p in self.props]

@@ -1241,6 +1241,41 @@ int fgpe_batch_step(fgpe_batch_t* b, int nsteps) {
     return FGPE_OK;
 }
 
+// fgpe_batch_step with device timing: CUDA events on the launch stream
+// before the first and after the last graph launch.  Only whole graphs are
+// timed, so nsteps must not leave a single-step remainder.
+int fgpe_batch_step_timed(fgpe_batch_t* b, int nsteps, double* device_ms) {
+    if (!b || !device_ms) return bfail(b, FGPE_E_ARG, "null argument");
+    if (nsteps < 2 || (nsteps % b->ksteps) == 1)
+        return bfail(b, FGPE_E_ARG, "timed batch steps need nsteps >= 2 and no single-step remainder");
+    for (fgpe_t* h : b->inst) BCK(cudaStreamSynchronize(h->st));
+    cudaEvent_t e0, e1;
+    BCK(cudaEventCreate(&e0));
+    BCK(cudaEventCreate(&e1));
+    int rc = FGPE_OK;
+    int left = nsteps;
+    cudaError_t err = cudaEventRecord(e0, b->origin);
+    while (err == cudaSuccess && rc == FGPE_OK && left > 0) {
+        int k = std::min(left, b->ksteps);
+        if (k == 1) k = 2;   // cannot happen: remainder 1 rejected above
+        if (!b->exec || b->exec_steps != k) rc = capture(b, k);
+        if (rc) break;
+        err = cudaGraphLaunch(b->exec, b->origin);
+        for (fgpe_t* h : b->inst) h->launches += (long long)k * (h->p.dim == 1 ? 1 : (h->p.dim == 2 ? 2 : 4));
+        left -= k;
+    }
+    if (err == cudaSuccess && rc == FGPE_OK) err = cudaEventRecord(e1, b->origin);
+    if (err == cudaSuccess && rc == FGPE_OK) err = cudaStreamSynchronize(b->origin);
+    float ms = 0.f;
+    if (err == cudaSuccess && rc == FGPE_OK) err = cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    BCK(err);
+    *device_ms = ms;
+    return FGPE_OK;
+}
+
 // Observables of every instance: out[i*OBS] = en, mz, conv (if requested and
 // available, else -1), then mu[M], rms[M], norm[M] (stride 3+3*M).
 int fgpe_batch_observables(fgpe_batch_t* b, double* out, int with_conv) {
@@ -1467,6 +1502,38 @@ int fno_adam(float* w, void* w_bf16, const float* g, float* m, float* v, long lo
 
 int fno_to_bf16(const float* x, void* y, long long n, void* stream) {
     fno::k_to_bf16<<<fno_grid(n), 256, 0, (cudaStream_t)stream>>>(x, (__nv_bfloat16*)y, n);
+    return fno_ck(cudaGetLastError());
+}
+
+#ifndef FNO_DENSE_GUARD
+#define FNO_DENSE_GUARD 0
+#endif
+static const size_t kDenseGuard = FNO_DENSE_GUARD;
+
+int fno_dense_tc(const void* w_bf16, int transpose_w, const float* x, const float* bias, float* z, float* h, int M,
+                 int K, long long n, int act, int* err_dev, void* stream) {
+    if (!w_bf16 || !x || !err_dev || (!z && !h)) { g_last_error = "null argument"; return FGPE_E_ARG; }
+    if (M < 1 || M > fno::tc::TM || K < 1 || K > 128 || n < 1) {
+        g_last_error = "dense layer needs 1 <= M <= 128 output and 1 <= K <= 128 input channels";
+        return FGPE_E_ARG;
+    }
+    const int KP = (K + 15) / 16 * 16;
+    // operand tiles plus alignment slack and a guard region behind them
+    const size_t smem = 1024 + (size_t)fno::tc::TM * KP * 2 + (size_t)KP * fno::tc::TN * 2 + kDenseGuard;
+    static bool attr_set[64] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(fno::k_dense_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)(1024 + (size_t)fno::tc::TM * 128 * 2 + (size_t)128 * fno::tc::TN * 2 +
+                                                   kDenseGuard));
+        if (e != cudaSuccess) return fno_ck(e);
+        attr_set[dev] = true;
+    }
+    const long long blocks = (n + fno::tc::TN - 1) / fno::tc::TN;
+    if (blocks > 0x7fffffffLL) { g_last_error = "too many columns"; return FGPE_E_ARG; }
+    fno::k_dense_tc<<<(unsigned)blocks, 128, smem, (cudaStream_t)stream>>>(
+        (const __nv_bfloat16*)w_bf16, transpose_w, x, bias, z, h, M, K, n, act, err_dev);
     return fno_ck(cudaGetLastError());
 }
 

@@ -198,4 +198,178 @@ __global__ void k_rbig_fold(const float* drb, float* drr, float* dri, long long 
     }
 }
 
+// ------------------------------------------------- tensor-core dense layer
+// z[m][n] = sum_k A(m,k) x[k][n] + bias[m],  h = GELU(z) or z,  for the
+// pointwise channel mixes (M, K <= 128 channels, n over all B*N*N points).
+// A(m,k) = W[m*K+k] (or W[k*M+m] when transposed), BF16; x is FP32 and is
+// rounded to BF16 on its way into shared memory; accumulation is FP32 in
+// tensor memory.  One CTA (4 warps) per 256 columns of n:
+//   - warp 0 allocates 256 TMEM columns (the 128 x 256 FP32 accumulator);
+//   - all threads stage A (K-major) and the x tile (N-major) in shared memory
+//     in the 8x8 core-matrix layout without swizzle;
+//   - thread 0 issues one tcgen05.mma (kind::f16, M=128, N=256, K=16) per 16
+//     channels and commits to an mbarrier;
+//   - each warp reads its 32 accumulator lanes with tcgen05.ld, adds the
+//     bias, applies GELU and stores rows of z and h.
+// The mbarrier wait is bounded; on expiry the CTA sets *err and skips its
+// stores (the accumulator is freed either way).
+namespace tc {
+constexpr int TN = 256;      // columns of n per CTA (accumulator width)
+constexpr int TM = 128;      // accumulator rows (M padded)
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Shared-memory matrix descriptor (no swizzle): start, leading and stride
+// byte offsets in 16-byte units, version 1 at bits 46-47.
+__device__ __forceinline__ uint64_t sdesc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFF);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+    d |= (uint64_t)1 << 46;
+    return d;
+}
+
+// Instruction descriptor: F32 accumulator, BF16 A and B, A K-major, B N-major,
+// N = TN, M = TM.
+__host__ __device__ constexpr uint32_t idesc_bf16() {
+    return (1u << 4) | (1u << 7) | (1u << 10) | (0u << 15) | (1u << 16) | ((uint32_t)(TN >> 3) << 17) |
+           ((uint32_t)(TM >> 4) << 24);
+}
+}  // namespace tc
+
+__global__ void __launch_bounds__(128, 1)
+k_dense_tc(const __nv_bfloat16* __restrict__ W, int transw, const float* __restrict__ x, const float* __restrict__ bias,
+           float* __restrict__ z, float* __restrict__ h, int M, int K, long long BS, int act, int* err) {
+    using namespace tc;
+    extern __shared__ __align__(1024) unsigned char smraw[];
+    const int KP = (K + 15) / 16 * 16;
+    // 1024-byte aligned operand tiles
+    const uint32_t base = smem_u32(smraw);
+    const uint32_t pad = (1024u - (base & 1023u)) & 1023u;
+    unsigned char* sA = smraw + pad;                          // TM x KP bf16, K-major cores
+    unsigned char* sB = sA + (size_t)TM * KP * 2;              // KP x TN bf16, N-major cores
+    __shared__ __align__(8) unsigned long long mbar;
+    __shared__ uint32_t tmem_slot;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const long long n0 = (long long)blockIdx.x * TN;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
+                     "r"(TN));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&mbar)), "r"(1));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    // A: element (m, k) -> core (k/8, m/8), row m%8, column k%8
+    for (int e = tid; e < TM * KP; e += 128) {
+        const int m = e / KP, k = e - (e / KP) * KP;
+        __nv_bfloat16 v = __float2bfloat16(0.f);
+        if (m < M && k < K) v = transw ? W[(size_t)k * M + m] : W[(size_t)m * K + k];
+        const int off = (((k >> 3) * (TM / 8) + (m >> 3)) << 7) + ((m & 7) << 4) + ((k & 7) << 1);
+        *(__nv_bfloat16*)(sA + off) = v;
+    }
+    // B: eight consecutive n of one k -> 16 bytes of core (k/8, n/8), row k%8
+    for (int e = tid; e < KP * (TN / 8); e += 128) {
+        const int k = e / (TN / 8), g = e - (e / (TN / 8)) * (TN / 8);
+        const long long n = n0 + g * 8;
+        float f[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) f[j] = 0.f;
+        if (k < K) {
+            const float* src = x + (size_t)k * BS + n;
+            if (n + 8 <= BS && ((((size_t)k * BS + n) & 3) == 0)) {
+                const float4 a = *(const float4*)src, b = *(const float4*)(src + 4);
+                f[0] = a.x; f[1] = a.y; f[2] = a.z; f[3] = a.w; f[4] = b.x; f[5] = b.y; f[6] = b.z; f[7] = b.w;
+            } else {
+#pragma unroll
+                for (int j = 0; j < 8; ++j) f[j] = (n + j < BS) ? src[j] : 0.f;
+            }
+        }
+        __nv_bfloat162 p[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) p[j] = __floats2bfloat162_rn(f[2 * j], f[2 * j + 1]);
+        const int off = (((k >> 3) * (TN / 8) + g) << 7) + ((k & 7) << 4);
+        *(uint4*)(sB + off) = *(uint4*)p;
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_slot;
+
+    if (tid == 0) {
+        const uint32_t idesc = idesc_bf16();
+        for (int s = 0; s < KP / 16; ++s) {
+            // K-major A: K chunks TM/8 cores apart, 8-row groups 128 B apart
+            const uint64_t da = sdesc(smem_u32(sA) + s * 2 * (TM / 8) * 128, (TM / 8) * 128, 128);
+            // N-major B: k groups TN/8 cores apart, 8-column groups 128 B apart
+            const uint64_t db = sdesc(smem_u32(sB) + s * 2 * (TN / 8) * 128, (TN / 8) * 128, 128);
+            const uint32_t acc = s > 0 ? 1u : 0u;
+            asm volatile(
+                "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+                "l"(da), "l"(db), "r"(idesc), "r"(acc));
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+            smem_u32(&mbar)));
+    }
+    // bounded wait for the accumulator (phase 0)
+    uint32_t done = 0;
+    for (long long it = 0; it < (1LL << 22) && !done; ++it) {
+        asm volatile(
+            "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, P1;\n\t}\n"
+            : "=r"(done)
+            : "r"(smem_u32(&mbar)), "r"(0));
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (!done) {
+        if (lane == 0) atomicExch(err, 1);
+    } else {
+        const int m = warp * 32 + lane;
+        const float bm = (bias && m < M) ? bias[m] : 0.f;
+        for (int cb = 0; cb < TN / 16; ++cb) {
+            uint32_t r[16];
+            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(cb * 16);
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+                : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (m < M) {
+                float v[16], g[16];
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    v[j] = __uint_as_float(r[j]) + bm;
+                    g[j] = act ? gelu_f(v[j]) : v[j];
+                }
+                const long long nb = n0 + cb * 16;
+                const size_t row = (size_t)m * BS + nb;
+                if (nb + 16 <= BS && (row & 3) == 0) {
+                    // each thread owns 64 contiguous bytes of its row
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        if (z) *(float4*)(z + row + 4 * q) = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+                        if (h) *(float4*)(h + row + 4 * q) = make_float4(g[4 * q], g[4 * q + 1], g[4 * q + 2], g[4 * q + 3]);
+                    }
+                } else {
+                    for (int j = 0; j < 16; ++j) {
+                        if (nb + j < BS) {
+                            if (z) z[row + j] = v[j];
+                            if (h) h[row + j] = g[j];
+                        }
+                    }
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TN));
+}
+
 }  // namespace fno

@@ -13,9 +13,10 @@ Network (width W, NM retained y modes, NA = 2 NM retained x modes):
           G_o = sum_c R_oc H_c per retained mode, w = 1 for ky = 0 else 2.
 
 Layout on the device: channel-major activations [C][B][N][N] (float32), so a
-pointwise channel mix is one GEMM over all B*N*N points.  Weights keep an
-FP32 master copy (Adam) and a BF16 copy that the GEMMs read; accumulation is
-FP32.  The spectral convolution is five GEMM stages over real/imaginary
+pointwise channel mix is one GEMM over all B*N*N points; those dense layers
+(and their input gradients) run on the tensor cores (fno_dense_tc: tcgen05,
+BF16 operands, FP32 accumulation in tensor memory, bias and GELU fused).
+Weights keep an FP32 master copy (Adam) and a BF16 copy that the GEMMs read.  The spectral convolution is five GEMM stages over real/imaginary
 planes (truncated DFTs as dense matrices), the per-mode channel mix a batched
 GEMM over the 2*NM*NM retained modes in the real block form
 [[Rr, -Ri], [Ri, Rr]].
@@ -32,7 +33,7 @@ import numpy as np
 from . import _abi
 
 FNO_EXPORTS = ("fno_gemm", "fno_bias_act", "fno_act_bwd", "fno_channel_sum", "fno_axpy", "fno_mse",
-               "fno_adam", "fno_to_bf16", "fno_rbig_build", "fno_rbig_fold")
+               "fno_adam", "fno_to_bf16", "fno_rbig_build", "fno_rbig_fold", "fno_dense_tc")
 
 _L = None
 
@@ -54,6 +55,7 @@ def lib():
         "fno_to_bf16": [vp, vp, ll, vp],
         "fno_rbig_build": [vp, vp, vp, ll, ip, ip, vp],
         "fno_rbig_fold": [vp, vp, vp, ll, ip, ip, vp],
+        "fno_dense_tc": [vp, ip, vp, vp, vp, vp, ip, ip, ll, ip, vp, vp],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -98,9 +100,13 @@ class FNO:
     matrices do), so a network trained at one resolution runs at another."""
 
     def __init__(self, n, batch, width=32, modes=16, layers=4, cin=7, hidden=128, cout=6, seed=0,
-                 params=None, device="cuda"):
+                 params=None, device="cuda", tensor_cores=True):
         import torch
         self.torch = torch
+        # dense (pointwise) layers on tcgen05 (BF16 operands, FP32 accumulation)
+        # when their channel counts fit one 128-row tile; else the FP32 GEMM
+        self.tensor_cores = tensor_cores
+        self.tc_err = torch.zeros(1, dtype=torch.int32, device=device)
         self.L = lib()
         self.n, self.B, self.W, self.NM, self.NA = n, batch, width, modes, 2 * modes
         self.layers, self.cin, self.hidden, self.cout = layers, cin, hidden, cout
@@ -238,10 +244,25 @@ class FNO:
                              beta, ctypes.c_void_p(C.data_ptr() + 4 * coff), sC[0], sC[1], sC[2], self._st())
         _ck(rc, "gemm")
 
-    def pointwise(self, wname, x, out, O, C, beta=0.0):
-        """out[O][BS] (+)= W[O][C] x[C][BS]"""
+    def _use_tc(self, M, K):
+        return self.tensor_cores and M <= 128 and K <= 128
+
+    def pointwise(self, wname, x, out, O, C, bias=None, act_out=None, act=False):
+        """out[O][BS] = W[O][C] x[C][BS] (+ bias); act_out = GELU(out) or out
+        when given."""
         BS = self.B * self.S
-        self.gemm(1, O, BS, C, self.pb[wname], (0, C, 1), x, (0, BS, 1), out, (0, BS, 1), beta=beta, a_bf16=True)
+        if self._use_tc(O, C):
+            _ck(self.L.fno_dense_tc(self._p(self.pb[wname]), 0, self._p(x), self._p(bias) if bias is not None else None,
+                                    self._p(out), self._p(act_out) if act_out is not None else None, O, C, BS,
+                                    int(act), self._p(self.tc_err), self._st()), "dense_tc")
+            return
+        self.gemm(1, O, BS, C, self.pb[wname], (0, C, 1), x, (0, BS, 1), out, (0, BS, 1), a_bf16=True)
+        if bias is not None or act_out is not None:
+            self.bias_act(out, act_out, bias, O, act)
+
+    def tc_error(self):
+        """True if a tensor-core layer's wait for its accumulator ran out."""
+        return bool(self.tc_err.item())
 
     def bias_act(self, z, h, bias, C, act):
         BS = self.B * self.S
@@ -302,18 +323,15 @@ class FNO:
         if a_host is not None:
             self.a.copy_(torch.from_numpy(np.ascontiguousarray(a_host.reshape(self.cin, -1))))
         W = self.W
-        self.pointwise("P", self.a, self.h[0], W, self.cin)
-        self.bias_act(self.h[0], None, self.p["bP"], W, False)
+        self.pointwise("P", self.a, self.h[0], W, self.cin, bias=self.p["bP"])
         for l in range(self.layers):
             z = self.zs[l]
             self.pointwise(f"W{l}", self.h[l], z, W, W)
             self.spectral(l, self.h[l], z)
             last = l == self.layers - 1
             self.bias_act(z, self.h[l + 1], self.p[f"b{l}"], W, not last)
-        self.pointwise("Q1", self.h[-1], self.u, self.hidden, W)
-        self.bias_act(self.u, self.q, self.p["c1"], self.hidden, True)
-        self.pointwise("Q2", self.q, self.out, self.cout, self.hidden)
-        self.bias_act(self.out, None, self.p["c2"], self.cout, False)
+        self.pointwise("Q1", self.h[-1], self.u, self.hidden, W, bias=self.p["c1"], act_out=self.q, act=True)
+        self.pointwise("Q2", self.q, self.out, self.cout, self.hidden, bias=self.p["c2"])
         return self.out
 
     def loss(self, target, want_grad=True):
@@ -336,10 +354,14 @@ class FNO:
         _ck(self.L.fno_channel_sum(self._p(self.g[gname]), self._p(dy), 1, O, self.B * self.S, 0.0, self._st()),
             "csum")
 
-    def _dinput(self, wname, dy, dx, O, C, beta=0.0):
-        """dx[C][BS] (+)= W^T dy"""
+    def _dinput(self, wname, dy, dx, O, C):
+        """dx[C][BS] = W^T dy"""
         BS = self.B * self.S
-        self.gemm(1, C, BS, O, self.pb[wname], (0, 1, C), dy, (0, BS, 1), dx, (0, BS, 1), beta=beta, a_bf16=True)
+        if self._use_tc(C, O):
+            _ck(self.L.fno_dense_tc(self._p(self.pb[wname]), 1, self._p(dy), None, self._p(dx), None, C, O, BS, 0,
+                                    self._p(self.tc_err), self._st()), "dense_tc")
+            return
+        self.gemm(1, C, BS, O, self.pb[wname], (0, 1, C), dy, (0, BS, 1), dx, (0, BS, 1), a_bf16=True)
 
     def backward(self):
         W, hid = self.W, self.hidden

@@ -161,6 +161,10 @@ const char *fgpe_batch_last_error(const fgpe_batch_t *b);
  * captured per graph launch (>= 2).  Non-positive values keep the setting. */
 int fgpe_batch_config(fgpe_batch_t *b, int width, int steps_per_graph);
 int fgpe_batch_step(fgpe_batch_t *b, int nsteps);
+/* As fgpe_batch_step, and device_ms receives the device time between CUDA
+ * events recorded on the batch's launch stream around its graph launches.
+ * nsteps >= 2 and nsteps % steps_per_graph != 1 (whole graphs only). */
+int fgpe_batch_step_timed(fgpe_batch_t *b, int nsteps, double *device_ms);
 /* For every instance i in order, 3+3*M_i doubles: EN, MZ, CONV (max|dphi|
  * of the last step, or -1), MU[M_i], RMS[M_i], NORM[M_i]. */
 int fgpe_batch_observables(fgpe_batch_t *b, double *out, int with_conv);

@@ -37,6 +37,14 @@ int fno_mse(const float *out, const float *target, float *dout, double *loss_dev
 int fno_adam(float *w, void *w_bf16, const float *g, float *m, float *v, long long n, float lr, float beta1,
              float beta2, float eps, int t, void *stream);
 int fno_to_bf16(const float *x, void *y, long long n, void *stream);
+/* Dense (pointwise channel-mixing) layer on the tensor cores (tcgen05):
+ *   z[m][j] = sum_k A(m,k) x[k][j] + bias[m],  h[m][j] = GELU(z) if act else z,
+ * A(m,k) = W[m*K+k] (W[k*M+m] if transpose_w), W bfloat16, x float32 (rounded
+ * to bfloat16 for the products), FP32 accumulation; 1 <= M, K <= 128,
+ * j < n.  z or h may be NULL (not both); bias may be NULL.  *err_dev (device
+ * int) is set to 1 if a CTA's wait for its accumulator ran out. */
+int fno_dense_tc(const void *w_bf16, int transpose_w, const float *x, const float *bias, float *z, float *h, int M,
+                 int K, long long n, int act, int *err_dev, void *stream);
 /* Per-mode complex channel mixing in real block form: from Rr, Ri [mode][O][C]
  * (float) build rbig [mode][2O][2C] = [[Rr,-Ri],[Ri,Rr]] in bfloat16, and fold
  * a gradient of that block form back to dRr = d00 + d11, dRi = d10 - d01. */

@@ -74,3 +74,25 @@ def test_batch_equals_individual(F, tmp_path):
     for i, p in enumerate(insts):
         b2[i].set_state(_guess(p, i))
     assert b2.autotune(trial_steps=4, cache_path=cache) == (w, k)
+
+
+def test_timed_batch_step(F):
+    """fgpe_batch_step_timed advances like fgpe_batch_step and reports the
+    device time of its graph launches; a single-step remainder is refused."""
+    from fortress_b200.batch import Batch
+    insts = _instances()[:3]
+    a, b = Batch(insts), Batch(insts)
+    for i, p in enumerate(insts):
+        phi = _guess(p, 10 + i)
+        for x in (a, b):
+            x[i].set_state(phi)
+            x[i].normt()
+    for x in (a, b):
+        x.config(width=2, steps_per_graph=4)
+    a.step(10)
+    ms = b.step_timed(10)          # graphs of 4, 4 and 2 steps
+    assert ms > 0
+    for i in range(len(insts)):
+        assert np.array_equal(a[i].state(), b[i].state())
+    with pytest.raises(F.FgpeError):
+        b.step_timed(9)            # 4 + 4 + 1
