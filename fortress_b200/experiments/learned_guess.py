@@ -135,6 +135,7 @@ def main():
     ap.add_argument("--n-train", type=int, default=64)
     ap.add_argument("--n-eval", type=int, default=256)
     ap.add_argument("--gen-steps", type=int, default=25000)
+    ap.add_argument("--gen-chunk", type=int, default=1024, help="instances per generation batch")
     ap.add_argument("--gen-dt", type=float, default=4e-3,
                     help="imaginary-time step of the training-data runs (a larger step relaxes faster; "
                          "its splitting error only shifts the targets slightly)")
@@ -156,13 +157,18 @@ def main():
     else:
         # FP32 bulk: its rounding floor keeps CONV above 1e-8, so the training
         # states are a fixed number of imaginary-time steps from the guess
-        insts = [instance(r, args.n_train, dt=args.gen_dt, precision="fp32") for r in ptr]
+        # (in batches of --gen-chunk instances)
         t0 = time.perf_counter()
-        r = solve(insts, [gaussian(p) for p in insts], tol=1e-8, max_steps=args.gen_steps, run_all=True)
-        tgt = states_to_target(r["states"]) * TARGET_SCALE
+        parts, conv = [], 0
+        for c0 in range(0, args.train, args.gen_chunk):
+            insts = [instance(r, args.n_train, dt=args.gen_dt, precision="fp32") for r in ptr[c0:c0 + args.gen_chunk]]
+            r = solve(insts, [gaussian(p) for p in insts], tol=1e-8, max_steps=args.gen_steps, run_all=True)
+            parts.append(states_to_target(r["states"]) * TARGET_SCALE)
+            conv += int((r["stop"] >= 0).sum())
+        tgt = np.concatenate(parts, axis=1)
         np.savez_compressed(data_path, t=tgt)
         print(json.dumps({"stage": "generate", "instances": args.train, "grid": args.n_train, "dt": args.gen_dt,
-                          "converged": int((r["stop"] >= 0).sum()), "steps": int(r["steps"]),
+                          "converged": conv, "steps": int(args.gen_steps),
                           "wall_s": time.perf_counter() - t0}), flush=True)
 
     # --------------------------------------------------------------- train
