@@ -56,6 +56,11 @@ struct fgpe_s {
     void* ctab = nullptr;
     double* h_small = nullptr;   // pinned, 64 doubles
     Launch row, col[3], k1, obsl;
+    // 1D lines too long for one block: N = n1*n2 split (k_r1d / k_c1d)
+    bool split1d = false;
+    int n1 = 0, n2 = 0;
+    Launch r1d, c1d;
+    const void *twn = nullptr, *tw1 = nullptr, *tw2 = nullptr;
     bool fast_row = false, fast_col[3] = {false, false, false};
     bool has_fast_row = false, has_fast_col[3] = {false, false, false};
     int fast_row_grid = 0, fast_col_grid[3] = {0, 0, 0};
@@ -150,6 +155,8 @@ template <typename T, int MS> cudaError_t set_smem_attrs() {
     cudaError_t e = allow_smem(k_row<T, MS>);
     if (e == cudaSuccess) e = allow_smem(k_col<T, MS>);
     if (e == cudaSuccess) e = allow_smem(k_1d<T, MS>);
+    if (e == cudaSuccess) e = allow_smem(k_r1d<T, MS>);
+    if (e == cudaSuccess) e = allow_smem(k_c1d<T, MS>);
     return e;
 }
 
@@ -382,6 +389,34 @@ void launch_1d(fgpe_t* h, int nsteps, void* snap_prev) {
     h->launches++;
 }
 
+template <typename T, int MS>
+Split1dArgs split_args(fgpe_t* h, int mode, void* snap) {
+    Split1dArgs a;
+    a.S = h->S; a.psi = h->psi; a.snap = snap;
+    a.twn = h->twn; a.tw1 = h->tw1; a.tw2 = h->tw2;
+    a.part = h->part; a.counter = h->counters; a.info = h->info;
+    a.n1 = h->n1; a.n2 = h->n2; a.mode = mode; a.tile = 0;
+    return a;
+}
+
+template <typename T, int MS>
+void launch_r1d(fgpe_t* h) {
+    Split1dArgs a = split_args<T, MS>(h, C1D_FULL, nullptr);
+    a.tile = h->r1d.tile;
+    ProfScope ps(h, 0);
+    k_r1d<T, MS><<<h->r1d.grid, h->r1d.T, h->r1d.smem, h->st>>>(h->sc, a);
+    h->launches++;
+}
+
+template <typename T, int MS>
+void launch_c1d(fgpe_t* h, int mode, void* snap) {
+    Split1dArgs a = split_args<T, MS>(h, mode, snap);
+    a.tile = h->c1d.tile;
+    ProfScope ps(h, 1);
+    k_c1d<T, MS><<<h->c1d.grid, h->c1d.T, h->c1d.smem, h->st>>>(h->sc, a);
+    h->launches++;
+}
+
 // dispatch on (precision, spin)
 #define DISPATCH(h, FN, ...)                                                  \
     do {                                                                      \
@@ -454,7 +489,8 @@ void launch_permute(fgpe_t* h, int to_natural) {
 int materialize(fgpe_t* h) {
     if (h->psi_valid) return FGPE_OK;
     if (!h->S_valid) return fail(h, FGPE_E_STATE, "no state set");
-    DISPATCH(h, launch_row, h, ROW_INV, nullptr);
+    if (h->split1d) DISPATCH(h, launch_c1d, h, C1D_INV, nullptr);
+    else DISPATCH(h, launch_row, h, ROW_INV, nullptr);
     CK(cudaGetLastError());
     h->psi_valid = true;
     return FGPE_OK;
@@ -601,6 +637,26 @@ int fgpe_create(const fgpe_params* pin, fgpe_t** out) {
         }
     }
 
+    // 1D lines whose spinor does not fit one block's shared memory: split
+    // N = n1*n2 (n1 the divisor nearest sqrt(N)) for the four-step transform
+    size_t off_tw1 = 0, off_tw2 = 0;
+    if (p.dim == 1 && (size_t)h->ms * padded_len(p.nx) * h->cs > 200 * 1024) {
+        int best = 0;
+        const double half = 0.5 * log((double)p.nx);
+        for (int d = 8; d <= p.nx / 8; ++d)
+            if (p.nx % d == 0 && (!best || fabs(log((double)d) - half) < fabs(log((double)best) - half))) best = d;
+        if (!best) { fgpe_destroy(h); return fail(nullptr, FGPE_E_ARG, "1D grid has no factorisation into two lines of >= 8"); }
+        h->split1d = true;
+        h->n1 = best;
+        h->n2 = p.nx / best;
+        plan_fft(h->n1, &c.px);
+        plan_fft(h->n2, &c.py);
+        off_tw1 = ct.size() / 2;
+        for (int t = 0; t < h->n1; ++t) { const double ang = -2.0 * kPi * t / h->n1; ct.push_back(cos(ang)); ct.push_back(sin(ang)); }
+        off_tw2 = ct.size() / 2;
+        for (int t = 0; t < h->n2; ++t) { const double ang = -2.0 * kPi * t / h->n2; ct.push_back(cos(ang)); ct.push_back(sin(ang)); }
+    }
+
     CK(cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking));
     h->own_stream = true;
     {
@@ -638,6 +694,11 @@ int fgpe_create(const fgpe_params* pin, fgpe_t** out) {
     c.twx = (char*)h->ctab + off_tw[0] * ces; c.twy = (char*)h->ctab + off_tw[1] * ces; c.twz = (char*)h->ctab + off_tw[2] * ces;
     c.kex = (char*)h->ctab + off_ke[0] * ces; c.key = (char*)h->ctab + off_ke[1] * ces; c.kez = (char*)h->ctab + off_ke[2] * ces;
     c.pvx = (char*)h->ctab + off_pv[0] * ces; c.pvy = (char*)h->ctab + off_pv[1] * ces; c.pvz = (char*)h->ctab + off_pv[2] * ces;
+    if (h->split1d) {
+        h->twn = c.twx;   // W_N^j of the whole line
+        h->tw1 = (char*)h->ctab + off_tw1 * ces;
+        h->tw2 = (char*)h->ctab + off_tw2 * ces;
+    }
 
     // ---- launch shapes
     const size_t budget = 100 * 1024;   // two blocks per SM
@@ -647,12 +708,30 @@ int fgpe_create(const fgpe_params* pin, fgpe_t** out) {
         const int lp = padded_len(p.nx);
         h->k1.smem = (size_t)ms * lp * h->cs;
         h->k1.T = 512;
-        if (h->k1.smem > hard) {
-            fgpe_destroy(h);
-            return fail(nullptr, FGPE_E_ARG, "1D grid too large for the single-block kernel (NX*M*bytes must fit 200 KB)");
-        }
     }
-    {
+    if (h->split1d) {
+        // row pass: R rows of n1 per block; column pass: TX columns of n2
+        int R = 1;
+        for (int r = 1; r <= 64; r *= 2) {
+            if (h->n2 % r || (size_t)ms * r * padded_len(h->n1) * h->cs > budget) break;
+            R = r;
+            if ((size_t)ms * r * h->n1 >= 2048) break;
+        }
+        int TX = 1;
+        for (int tx = 1; tx <= 16; tx *= 2) {
+            if (h->n1 % tx || (size_t)ms * tx * padded_len(h->n2) * h->cs > budget) break;
+            TX = tx;
+            if ((size_t)tx * h->cs >= 32) break;
+        }
+        h->r1d.tile = R; h->r1d.T = 256; h->r1d.smem = (size_t)ms * R * padded_len(h->n1) * h->cs;
+        h->r1d.grid = dim3(h->n2 / R);
+        h->c1d.tile = TX; h->c1d.T = 256; h->c1d.smem = (size_t)ms * TX * padded_len(h->n2) * h->cs;
+        h->c1d.grid = dim3(h->n1 / TX);
+        if (h->r1d.smem > hard || h->c1d.smem > hard) {
+            fgpe_destroy(h);
+            return fail(nullptr, FGPE_E_ARG, "1D grid too large for the split transform");
+        }
+    } else {
         // row pass: R rows per block, R | NY*NZ
         const int rows = p.ny * p.nz;
         const int lp = padded_len(p.nx);
@@ -714,7 +793,9 @@ int fgpe_create(const fgpe_params* pin, fgpe_t** out) {
     cudaGetLastError();   // clear any attribute/occupancy probe error
     h->obsl.grid = dim3((unsigned)((h->npts + 255) / 256));
     const size_t nq = 3 * ms + 3;
-    const size_t npart = std::max<size_t>((size_t)h->obsl.grid.x * nq, (size_t)std::max<int>(h->row.grid.x, h->fast_row_grid) * ms) + 64;
+    const size_t npart = std::max<size_t>(std::max<size_t>((size_t)h->obsl.grid.x * nq,
+                                                           (size_t)std::max<int>(h->row.grid.x, h->fast_row_grid) * ms),
+                                          (size_t)h->c1d.grid.x * ms) + 64;
     CK(cudaMalloc(&h->part, npart * sizeof(double)));
     CK(cudaMalloc(&h->info, 4 * INFO_LEN * sizeof(double)));
     h->info_prev = h->info + INFO_LEN;
@@ -835,7 +916,7 @@ int fgpe_step_ex(fgpe_t* h, int nsteps, int flags) {
     if (!h->has_state) return fail(h, FGPE_E_STATE, "no state set");
     if (nsteps <= 0) return FGPE_OK;
     const bool snap = !(flags & FGPE_STEP_NO_SNAPSHOT);
-    if (h->p.dim == 1) {
+    if (h->p.dim == 1 && !h->split1d) {
         // the state of a 1D handle always lives in psi
         int done = 0;
         while (done < nsteps) {
@@ -859,7 +940,8 @@ int fgpe_step_ex(fgpe_t* h, int nsteps, int flags) {
     }
     if (!h->S_valid) {
         if (!h->psi_valid) return fail(h, FGPE_E_STATE, "no state set");
-        DISPATCH(h, launch_row, h, ROW_FWD, nullptr);
+        if (h->split1d) DISPATCH(h, launch_c1d, h, C1D_FWD, nullptr);
+        else DISPATCH(h, launch_row, h, ROW_FWD, nullptr);
         CK(cudaGetLastError());
         h->S_valid = true;
     }
@@ -874,6 +956,19 @@ int fgpe_step_ex(fgpe_t* h, int nsteps, int flags) {
     }
     h->psi_valid = false;
     for (int s = 0; s < nsteps; ++s) {
+        if (h->split1d) {
+            // long 1D line: spectral row pass, then the real-space column pass
+            void* sn = nullptr;
+            if (snap && s == nsteps - 1) sn = h->psi;
+            if (snap && s == nsteps - 2) sn = h->prev;
+            DISPATCH(h, launch_r1d, h);
+            DISPATCH(h, launch_c1d, h, C1D_FULL, sn);
+            if (snap && s == nsteps - 2) {
+                CK(cudaMemcpyAsync(h->info_prev, h->info, INFO_LEN * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
+                h->prev_valid = true;
+            }
+            continue;
+        }
         if (h->p.dim == 2) {
             DISPATCH(h, launch_col, h, 1, COL_SCALE | COL_FWD | COL_KOP | COL_INV);
         } else {
@@ -992,6 +1087,8 @@ int fgpe_apply_op(fgpe_t* h, int op) {
     h->launches++;
     const double ones[5] = {1.0, 1.0, 1.0, 1.0, 1.0};   // pageable source: staged before the call returns
     CK(cudaMemcpyAsync(h->info + INFO_SC, ones, sizeof(ones), cudaMemcpyHostToDevice, h->st));
+    if (h->split1d && (op == FGPE_OP_FFT || op == FGPE_OP_BFT))
+        return fail(h, FGPE_E_ARG, "the unfused FFT/BFT need the whole 1D line in one block (this line is split)");
     switch (op) {
         case FGPE_OP_FFT: {
             void* keep = h->S;
@@ -1234,7 +1331,7 @@ int fgpe_batch_step(fgpe_batch_t* b, int nsteps) {
         }
         if (!b->exec || b->exec_steps != k) { int r = capture(b, k); if (r) return r; }
         BCK(cudaGraphLaunch(b->exec, b->origin));
-        for (fgpe_t* h : b->inst) h->launches += (long long)k * (h->p.dim == 1 ? 1 : (h->p.dim == 2 ? 2 : 4));
+        for (fgpe_t* h : b->inst) h->launches += (long long)k * (h->p.dim == 1 ? (h->split1d ? 2 : 1) : (h->p.dim == 2 ? 2 : 4));
         left -= k;
     }
     BCK(cudaStreamSynchronize(b->origin));
@@ -1261,7 +1358,7 @@ int fgpe_batch_step_timed(fgpe_batch_t* b, int nsteps, double* device_ms) {
         if (!b->exec || b->exec_steps != k) rc = capture(b, k);
         if (rc) break;
         err = cudaGraphLaunch(b->exec, b->origin);
-        for (fgpe_t* h : b->inst) h->launches += (long long)k * (h->p.dim == 1 ? 1 : (h->p.dim == 2 ? 2 : 4));
+        for (fgpe_t* h : b->inst) h->launches += (long long)k * (h->p.dim == 1 ? (h->split1d ? 2 : 1) : (h->p.dim == 2 ? 2 : 4));
         left -= k;
     }
     if (err == cudaSuccess && rc == FGPE_OK) err = cudaEventRecord(e1, b->origin);

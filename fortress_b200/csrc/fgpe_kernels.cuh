@@ -221,6 +221,127 @@ k_col(StepConst c, ColArgs a) {
     }
 }
 
+// ---------------------------------------------------- long 1D lines
+// Row pass of a step (rows p2 of Q, N1 points each): scale by sc_m/N, F_N1,
+// KE and SOC at the 1D frequency k = k2 + N2*k1, F_N1^-1.  c.px/c.fx are the
+// N1 transform's plan and position map, c.py/c.fy the N2 ones.
+template <typename T, int MS>
+__global__ void __launch_bounds__(256)
+k_r1d(StepConst c, Split1dArgs a) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cx<T>* sm = (cx<T>*)smraw;
+    const int n1 = a.n1, R = a.tile;
+    const int lp = padded_len(n1);
+    const RowMap mp{lp};
+    const int row0 = blockIdx.x * R;
+    const long long np = c.npts;
+    cx<T>* S = (cx<T>*)a.S;
+    T fac[MS];
+#pragma unroll
+    for (int m = 0; m < MS; ++m) fac[m] = (T)(a.info[INFO_SC + m] / (double)np);
+    const int nel = MS * R * n1;
+    for (int idx = threadIdx.x; idx < nel; idx += blockDim.x) {
+        const int x = idx % n1, q = idx / n1, r = q % R, m = q / R;
+        sm[(m * R + r) * lp + pad_idx(x)] = cscale(S[(size_t)m * np + (size_t)(row0 + r) * n1 + x], fac[m]);
+    }
+    __syncthreads();
+    block_fft<T, false>(sm, mp, MS * R, c.px, (const cx<T>*)a.tw1);
+    for (int p = threadIdx.x; p < R * n1; p += blockDim.x) {
+        const int x = p % n1, r = p / n1;
+        const int k = c.fy[row0 + r] + a.n2 * c.fx[x];
+        cx<T> v[MS];
+#pragma unroll
+        for (int m = 0; m < MS; ++m) v[m] = sm[(m * R + r) * lp + pad_idx(x)];
+        apply_ke<T, MS>(c, k, 0, 0, v);
+        apply_soc<T, MS>(c, c.kx[k], 0.0, v);
+#pragma unroll
+        for (int m = 0; m < MS; ++m) sm[(m * R + r) * lp + pad_idx(x)] = v[m];
+    }
+    __syncthreads();
+    block_fft<T, true>(sm, mp, MS * R, c.px, (const cx<T>*)a.tw1);
+    for (int idx = threadIdx.x; idx < nel; idx += blockDim.x) {
+        const int x = idx % n1, q = idx / n1, r = q % R, m = q / R;
+        S[(size_t)m * np + (size_t)(row0 + r) * n1 + x] = sm[(m * R + r) * lp + pad_idx(x)];
+    }
+}
+
+// Column pass (columns n1, N2 points each, TX adjacent columns per block).
+//  C1D_FULL: conj twiddle, F_N2^-1 (real space), SE, SP, NORMC partials
+//            (+ snapshot), F_N2, twiddle; the last block finishes NORMC and
+//            the next scales.
+//  C1D_FWD : psi (real space) -> Q (prologue).
+//  C1D_INV : Q -> psi = x (export; the pending scales stay in info).
+template <typename T, int MS>
+__global__ void __launch_bounds__(256)
+k_c1d(StepConst c, Split1dArgs a) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cx<T>* sm = (cx<T>*)smraw;
+    __shared__ double red[32 * (MS + 1)];
+    __shared__ double bsum[MS];
+    const int n1 = a.n1, n2 = a.n2, TX = a.tile;
+    const int lpn = padded_len(n2);
+    const ColMap mp{TX, lpn};
+    const int x0 = blockIdx.x * TX;
+    const long long np = c.npts;
+    const cx<T>* twn = (const cx<T>*)a.twn;
+    const cx<T>* tw2 = (const cx<T>*)a.tw2;
+    cx<T>* S = (cx<T>*)a.S;
+    const int nel = MS * n2 * TX;
+    const cx<T>* src = a.mode == C1D_FWD ? (const cx<T>*)a.psi : S;
+    for (int idx = threadIdx.x; idx < nel; idx += blockDim.x) {
+        const int t = idx % TX, q = idx / TX, e = q % n2, m = q / n2;
+        cx<T> v = src[(size_t)m * np + (size_t)e * n1 + x0 + t];
+        if (a.mode != C1D_FWD) v = cmulc(v, twn[(size_t)(x0 + t) * c.fy[e]]);   // conj twiddle
+        sm[(m * lpn + pad_idx(e)) * TX + t] = v;
+    }
+    __syncthreads();
+    if (a.mode != C1D_FWD) block_fft<T, true>(sm, mp, MS * TX, c.py, tw2);
+    if (a.mode == C1D_INV) {
+        const T inv = (T)(1.0 / n2);
+        cx<T>* dst = (cx<T>*)a.psi;
+        for (int idx = threadIdx.x; idx < nel; idx += blockDim.x) {
+            const int t = idx % TX, q = idx / TX, e = q % n2, m = q / n2;
+            dst[(size_t)m * np + (size_t)e * n1 + x0 + t] = cscale(sm[(m * lpn + pad_idx(e)) * TX + t], inv);
+        }
+        return;
+    }
+    if (a.mode == C1D_FULL) {
+        double acc[MS];
+#pragma unroll
+        for (int m = 0; m < MS; ++m) acc[m] = 0.0;
+        cx<T>* snap = (cx<T>*)a.snap;
+        for (int p = threadIdx.x; p < n2 * TX; p += blockDim.x) {
+            const int t = p % TX, e = p / TX;
+            const int x = x0 + t + n1 * e;             // 1D grid index
+            cx<T> v[MS];
+#pragma unroll
+            for (int m = 0; m < MS; ++m) v[m] = sm[(m * lpn + pad_idx(e)) * TX + t];
+            const cx<T> eV = pot_phase<T>(c, x, 0, 0);
+            apply_se<T, MS>(c, v);
+            apply_sp<T, MS>(c, eV, v);
+            const double w = c.wx[x];
+#pragma unroll
+            for (int m = 0; m < MS; ++m) {
+                acc[m] += w * ((double)v[m].x * (double)v[m].x + (double)v[m].y * (double)v[m].y);
+                sm[(m * lpn + pad_idx(e)) * TX + t] = v[m];
+            }
+            if (snap) {
+#pragma unroll
+                for (int m = 0; m < MS; ++m) snap[(size_t)m * np + x] = v[m];
+            }
+        }
+        block_sum<MS>(acc, red, bsum);
+        if (threadIdx.x < MS) a.part[(size_t)blockIdx.x * MS + threadIdx.x] = bsum[threadIdx.x];
+        finish_norms<MS>(c, a.part, a.counter, a.info, red);
+        __syncthreads();
+    }
+    block_fft<T, false>(sm, mp, MS * TX, c.py, tw2);
+    for (int idx = threadIdx.x; idx < nel; idx += blockDim.x) {
+        const int t = idx % TX, q = idx / TX, e = q % n2, m = q / n2;
+        S[(size_t)m * np + (size_t)e * n1 + x0 + t] = cmul(sm[(m * lpn + pad_idx(e)) * TX + t], twn[(size_t)(x0 + t) * c.fy[e]]);
+    }
+}
+
 // ------------------------------------------------------------- 1D steps
 // One block holds PHI(NX, MS) and runs nsteps full split steps
 // (cgpe1d.f90:434-472); psi is normalised in place every imaginary step so

@@ -47,6 +47,26 @@ struct ColArgs {
     int n_other;       // number of positions along the third axis (1 in 2D)
 };
 
+// Long 1D lines, N = N1*N2 points, handled as an N2 x N1 array (x = n1 + N1*n2)
+// in two passes per step (four-step transform): the state between passes is
+// Q[p2][n1] = W_N^(n1*k2) * sum_n2 x[n1 + N1*n2] W_N2^(n2*k2), row p2 holding
+// the column frequency k2 = fy[p2].
+enum { C1D_FULL = 0, C1D_FWD = 1, C1D_INV = 2 };
+struct Split1dArgs {
+    void* S;           // Q (in/out)
+    void* psi;         // real space (C1D_FWD source, C1D_INV target)
+    void* snap;        // C1D_FULL: optional real-space snapshot target
+    const void* twn;   // W_N^j, j < N
+    const void* tw1;   // twiddles of the N1 transform
+    const void* tw2;   // twiddles of the N2 transform
+    double* part;
+    unsigned* counter;
+    double* info;
+    int n1, n2;
+    int tile;          // rows (row pass) or columns (column pass) per block
+    int mode;
+};
+
 struct OneDArgs {
     void* psi;
     void* snap_prev;
