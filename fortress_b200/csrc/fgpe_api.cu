@@ -106,21 +106,6 @@ bool plan_fft(int n, FftPlan* pl) {
     return true;
 }
 
-// Largest per-thread load of a pass: nlines*n elements split so that each
-// thread keeps at most 16 complex values (15 for radix 3 and 5).
-int threads_needed(int nel, const FftPlan& pl) {
-    int need = 32;
-    for (int i = 0; i < pl.nf; ++i) {
-        const int R = pl.r[i];
-        const int K = 16 / R;
-        const int nb = nel / R;
-        need = std::max(need, (nb + K - 1) / K);
-    }
-    return need;
-}
-
-int round32(int x) { return (x + 31) / 32 * 32; }
-
 // simpson.f90:4-21 applied to unit vectors: the weight of every node.
 std::vector<double> simpson_weights(int n, double dx) {
     std::vector<double> w(n, 0.0);

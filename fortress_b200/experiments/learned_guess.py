@@ -144,65 +144,75 @@ def main():
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--max-steps", type=int, default=200000)
     ap.add_argument("--out", default="/tmp/learned_guess", help="training data and trained parameters")
+    ap.add_argument("--params", default=None, help="trained parameters (.npz) to evaluate instead of training")
+    ap.add_argument("--save-params", default=None, help="also write the trained parameters here")
+    ap.add_argument("--fp32-tol", type=float, default=1e-6,
+                    help="stop rule of the FP32 stage of the learned+FP32 arm (its rounding floor is above 1e-8)")
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)
     import torch
     from fortress_b200 import fno as FN
 
-    # ---------------------------------------------------------------- data
-    ptr, pho = box(args.train, 5), box(args.heldout, 6)
-    data_path = os.path.join(args.out, f"train_{args.train}_{args.n_train}_{args.gen_steps}_{args.gen_dt}.npz")
-    if os.path.exists(data_path):
-        tgt = np.load(data_path)["t"]
+    if args.params is not None:
+        pfin = {k: np.asarray(v, np.float64) for k, v in np.load(args.params).items()}
+        ptr, pho = None, box(args.heldout, 6)
     else:
-        # FP32 bulk: its rounding floor keeps CONV above 1e-8, so the training
-        # states are a fixed number of imaginary-time steps from the guess
-        # (in batches of --gen-chunk instances)
-        t0 = time.perf_counter()
-        parts, conv = [], 0
-        for c0 in range(0, args.train, args.gen_chunk):
-            insts = [instance(r, args.n_train, dt=args.gen_dt, precision="fp32") for r in ptr[c0:c0 + args.gen_chunk]]
-            r = solve(insts, [gaussian(p) for p in insts], tol=1e-8, max_steps=args.gen_steps, run_all=True)
-            parts.append(states_to_target(r["states"]) * TARGET_SCALE)
-            conv += int((r["stop"] >= 0).sum())
-        tgt = np.concatenate(parts, axis=1)
-        np.savez_compressed(data_path, t=tgt)
-        print(json.dumps({"stage": "generate", "instances": args.train, "grid": args.n_train, "dt": args.gen_dt,
-                          "converged": conv, "steps": int(args.gen_steps),
-                          "wall_s": time.perf_counter() - t0}), flush=True)
+        # ---------------------------------------------------------------- data
+        ptr, pho = box(args.train, 5), box(args.heldout, 6)
+        data_path = os.path.join(args.out, f"train_{args.train}_{args.n_train}_{args.gen_steps}_{args.gen_dt}.npz")
+        if os.path.exists(data_path):
+            tgt = np.load(data_path)["t"]
+        else:
+            # FP32 bulk: its rounding floor keeps CONV above 1e-8, so the training
+            # states are a fixed number of imaginary-time steps from the guess
+            # (in batches of --gen-chunk instances)
+            t0 = time.perf_counter()
+            parts, conv = [], 0
+            for c0 in range(0, args.train, args.gen_chunk):
+                insts = [instance(r, args.n_train, dt=args.gen_dt, precision="fp32") for r in ptr[c0:c0 + args.gen_chunk]]
+                r = solve(insts, [gaussian(p) for p in insts], tol=1e-8, max_steps=args.gen_steps, run_all=True)
+                parts.append(states_to_target(r["states"]) * TARGET_SCALE)
+                conv += int((r["stop"] >= 0).sum())
+            tgt = np.concatenate(parts, axis=1)
+            np.savez_compressed(data_path, t=tgt)
+            print(json.dumps({"stage": "generate", "instances": args.train, "grid": args.n_train, "dt": args.gen_dt,
+                              "converged": conv, "steps": int(args.gen_steps),
+                              "wall_s": time.perf_counter() - t0}), flush=True)
 
-    # --------------------------------------------------------------- train
-    a_all = FN.input_channels(np.array([FN.normalise_params(*row) for row in ptr]), args.n_train)
-    B = args.batch
-    net = FN.FNO(args.n_train, B, seed=7)
-    nb = args.train // B
-    t0 = time.perf_counter()
-    rng = np.random.default_rng(8)
-    tgt_dev = torch.tensor(tgt.reshape(6, args.train, -1), device="cuda")
-    a_dev = torch.tensor(a_all.reshape(7, args.train, -1), device="cuda")
-    losses = []
-    steps_total = args.epochs * nb
-    it = 0
-    for ep in range(args.epochs):
-        perm = torch.tensor(rng.permutation(args.train), device="cuda")
-        tot = torch.zeros(1, dtype=torch.float64, device="cuda")
-        for k in range(nb):
-            idx = perm[k * B:(k + 1) * B]
-            net.a.copy_(a_dev[:, idx, :].reshape(7, -1))
-            tb = tgt_dev[:, idx, :].reshape(6, -1).contiguous()
-            net.forward()
-            tot += net.loss(tb)
-            net.backward()
-            lr = args.lr * 0.5 * (1 + np.cos(np.pi * it / steps_total))
-            net.adam(lr=lr)
-            it += 1
-        losses.append(float(tot.item()) / nb)
-    torch.cuda.synchronize()
-    train_s = time.perf_counter() - t0
-    pfin = net.params_numpy()
-    np.savez_compressed(os.path.join(args.out, "fno_params.npz"), **{k: v.astype(np.float32) for k, v in pfin.items()})
-    print(json.dumps({"stage": "train", "samples": args.train, "grid": args.n_train, "epochs": args.epochs,
-                      "batch": B, "wall_s": train_s, "loss_first": losses[0], "loss_last": losses[-1]}), flush=True)
+        # --------------------------------------------------------------- train
+        a_all = FN.input_channels(np.array([FN.normalise_params(*row) for row in ptr]), args.n_train)
+        B = args.batch
+        net = FN.FNO(args.n_train, B, seed=7)
+        nb = args.train // B
+        t0 = time.perf_counter()
+        rng = np.random.default_rng(8)
+        tgt_dev = torch.tensor(tgt.reshape(6, args.train, -1), device="cuda")
+        a_dev = torch.tensor(a_all.reshape(7, args.train, -1), device="cuda")
+        losses = []
+        steps_total = args.epochs * nb
+        it = 0
+        for ep in range(args.epochs):
+            perm = torch.tensor(rng.permutation(args.train), device="cuda")
+            tot = torch.zeros(1, dtype=torch.float64, device="cuda")
+            for k in range(nb):
+                idx = perm[k * B:(k + 1) * B]
+                net.a.copy_(a_dev[:, idx, :].reshape(7, -1))
+                tb = tgt_dev[:, idx, :].reshape(6, -1).contiguous()
+                net.forward()
+                tot += net.loss(tb)
+                net.backward()
+                lr = args.lr * 0.5 * (1 + np.cos(np.pi * it / steps_total))
+                net.adam(lr=lr)
+                it += 1
+            losses.append(float(tot.item()) / nb)
+        torch.cuda.synchronize()
+        train_s = time.perf_counter() - t0
+        pfin = net.params_numpy()
+        np.savez_compressed(os.path.join(args.out, "fno_params.npz"), **{k: v.astype(np.float32) for k, v in pfin.items()})
+        print(json.dumps({"stage": "train", "samples": args.train, "grid": args.n_train, "epochs": args.epochs,
+                          "batch": B, "wall_s": train_s, "loss_first": losses[0], "loss_last": losses[-1]}), flush=True)
+        if args.save_params:
+            np.savez_compressed(args.save_params, **{k: v.astype(np.float32) for k, v in pfin.items()})
 
     # ---------------------------------------------------------------- eval
     ne = args.n_eval
@@ -223,8 +233,13 @@ def main():
     infer_s = time.perf_counter() - t0
     g_run = solve(insts, [gaussian(p) for p in insts], max_steps=args.max_steps, run_all=True)
     l_run = solve(insts, guesses, max_steps=args.max_steps, run_all=True)
-    # E*: the lower of the two final energies (both arms ran max_steps)
-    e_star = np.minimum(g_run["traj"][-1], l_run["traj"][-1])
+    # learned + FP32: the FP32 bulk path until its own stop rule at --fp32-tol
+    # (its rounding floor keeps CONV above 1e-8), then FP64 from that state
+    insts32 = [instance(r, ne, precision="fp32") for r in pho]
+    a32 = solve(insts32, guesses, tol=args.fp32_tol, max_steps=args.max_steps)
+    h64 = solve(insts, a32["states"], max_steps=args.max_steps, run_all=True)
+    # E*: the lowest of the final energies (the FP64 arms ran max_steps)
+    e_star = np.minimum(np.minimum(g_run["traj"][-1], l_run["traj"][-1]), h64["traj"][-1])
     res = {}
     for name, r in (("gaussian", g_run), ("learned", l_run)):
         reach = first_within(r["traj"], r["stp"], e_star, 1e-8).astype(float)
@@ -238,6 +253,20 @@ def main():
                          batch_ms_per_step=1e3 * per_step,
                          wall_to_reach_all_s=float(np.nanmax(reach) * per_step) if np.any(~np.isnan(reach)) else None,
                          final_rel_above_estar_max=float(np.max((r["traj"][-1] - e_star) / np.abs(e_star))))
+    # the hybrid arm: per instance FP32 steps to its stop rule, then FP64 steps
+    s32 = a32["stop"].astype(float); s32[s32 < 0] = np.nan
+    s64 = h64["stop"].astype(float); s64[s64 < 0] = np.nan
+    r64 = first_within(h64["traj"], h64["stp"], e_star, 1e-8).astype(float); r64[r64 < 0] = np.nan
+    t32, t64 = a32["wall"] / a32["steps"], h64["wall"] / h64["steps"]
+    res["learned_fp32_then_fp64"] = dict(
+        fp32_steps_median=float(np.nanmedian(s32)), fp32_never=int(np.isnan(s32).sum()),
+        fp64_stop_median=float(np.nanmedian(s64)), fp64_stop_never=int(np.isnan(s64).sum()),
+        fp64_reach_median=float(np.nanmedian(r64)), fp64_reach_never=int(np.isnan(r64).sum()),
+        batch_ms_per_step_fp32=1e3 * t32, batch_ms_per_step_fp64=1e3 * t64,
+        stop_time_median_batch_ms=float(np.nanmedian(s32 * t32 + s64 * t64) * 1e3),
+        final_rel_above_estar_max=float(np.max((h64["traj"][-1] - e_star) / np.abs(e_star))))
+    for name in ("gaussian", "learned"):
+        res[name]["stop_time_median_batch_ms"] = res[name]["stop_median"] * res[name]["batch_ms_per_step"]
     print(json.dumps({"stage": "compare", "heldout": args.heldout, "grid": ne, "tol": 1e-8,
                       "steps_run": args.max_steps, "inference_s": infer_s, **res,
                       "reach_median_ratio": res["gaussian"]["reach_median"] / res["learned"]["reach_median"],
