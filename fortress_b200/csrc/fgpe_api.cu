@@ -61,6 +61,11 @@ struct fgpe_s {
     int n1 = 0, n2 = 0;
     Launch r1d, c1d;
     const void *twn = nullptr, *tw1 = nullptr, *tw2 = nullptr;
+    // CUDA graph of kBulkSteps whole steps without snapshots, replayed for
+    // the bulk of multi-step calls (built on first use, dropped when the
+    // kernel choice changes)
+    cudaGraphExec_t bulk = nullptr;
+    bool bulk_off = false;
     bool fast_row = false, fast_col[3] = {false, false, false};
     bool has_fast_row = false, has_fast_col[3] = {false, false, false};
     int fast_row_grid = 0, fast_col_grid[3] = {0, 0, 0};
@@ -622,10 +627,16 @@ int fgpe_create(const fgpe_params* pin, fgpe_t** out) {
         }
     }
 
-    // 1D lines whose spinor does not fit one block's shared memory: split
-    // N = n1*n2 (n1 the divisor nearest sqrt(N)) for the four-step transform
+    // 1D lines whose spinor needs more than 96 KB of shared memory: split
+    // N = n1*n2 (n1 the divisor nearest sqrt(N)) for the four-step transform.
+    // Above that size the single-block kernel (one SM) is the slower one: at
+    // 2048 spin-2 FP64 points a step takes 52 us there and 26-31 us split.
     size_t off_tw1 = 0, off_tw2 = 0;
-    if (p.dim == 1 && (size_t)h->ms * padded_len(p.nx) * h->cs > 200 * 1024) {
+    const size_t line1d = (size_t)h->ms * padded_len(p.nx) * h->cs;
+    const bool must_split = p.dim == 1 && line1d > 200 * 1024;
+    const bool prefer_split = p.dim == 1 && (line1d > 96 * 1024 || p.kernels == FGPE_KERNELS_SPLIT_1D) &&
+                              p.kernels != FGPE_KERNELS_SINGLE_1D;
+    if (must_split || prefer_split) {
         int best = 0;
         const double half = 0.5 * log((double)p.nx);
         for (int d = 8; d <= p.nx / 8; ++d)
@@ -806,6 +817,7 @@ int fgpe_create(const fgpe_params* pin, fgpe_t** out) {
 int fgpe_destroy(fgpe_t* h) {
     if (!h) return FGPE_OK;
     if (h->st) cudaStreamSynchronize(h->st);
+    if (h->bulk) cudaGraphExecDestroy(h->bulk);
     cudaFree(h->S); cudaFree(h->psi); cudaFree(h->prev); cudaFree(h->stage);
     cudaFree(h->dtab); cudaFree(h->ctab); cudaFree(h->part); cudaFree(h->info);
     cudaFree(h->counters); cudaFree(h->pmap);
@@ -896,6 +908,8 @@ int fgpe_get_state_device(fgpe_t* h, void* phi_dev) {
     return export_to(h, phi_dev, cudaMemcpyDeviceToDevice);
 }
 
+constexpr int kBulkSteps = 16;
+
 int fgpe_step_ex(fgpe_t* h, int nsteps, int flags) {
     if (!h) return fail(h, FGPE_E_ARG, "null handle");
     if (!h->has_state) return fail(h, FGPE_E_STATE, "no state set");
@@ -940,19 +954,12 @@ int fgpe_step_ex(fgpe_t* h, int nsteps, int flags) {
         h->prev_valid = true;
     }
     h->psi_valid = false;
-    for (int s = 0; s < nsteps; ++s) {
+    // the passes of one step; sn: real-space snapshot target of the step
+    auto launch_step = [&](void* sn) {
         if (h->split1d) {
-            // long 1D line: spectral row pass, then the real-space column pass
-            void* sn = nullptr;
-            if (snap && s == nsteps - 1) sn = h->psi;
-            if (snap && s == nsteps - 2) sn = h->prev;
             DISPATCH(h, launch_r1d, h);
             DISPATCH(h, launch_c1d, h, C1D_FULL, sn);
-            if (snap && s == nsteps - 2) {
-                CK(cudaMemcpyAsync(h->info_prev, h->info, INFO_LEN * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
-                h->prev_valid = true;
-            }
-            continue;
+            return;
         }
         if (h->p.dim == 2) {
             DISPATCH(h, launch_col, h, 1, COL_SCALE | COL_FWD | COL_KOP | COL_INV);
@@ -961,10 +968,48 @@ int fgpe_step_ex(fgpe_t* h, int nsteps, int flags) {
             DISPATCH(h, launch_col, h, 2, COL_FWD | COL_KOP | COL_INV);
             DISPATCH(h, launch_col, h, 1, COL_INV);
         }
+        DISPATCH(h, launch_row, h, ROW_FULL, sn);
+    };
+    // bulk steps (no snapshot: all but the last two of a snapshotting call)
+    // as replays of a captured graph, unless profiling or already capturing
+    int s = 0;
+    const int tail = snap ? 2 : 0;
+    if (!h->prof && !h->bulk_off && nsteps - tail >= 2 * kBulkSteps) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        CK(cudaStreamIsCapturing(h->st, &cs));
+        if (cs == cudaStreamCaptureStatusNone) {
+            if (!h->bulk) {
+                const long long l0 = h->launches;
+                cudaGraph_t g = nullptr;
+                cudaError_t e = cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal);
+                if (e == cudaSuccess) {
+                    for (int k = 0; k < kBulkSteps; ++k) launch_step(nullptr);
+                    e = cudaStreamEndCapture(h->st, &g);
+                }
+                if (e == cudaSuccess) e = cudaGraphInstantiate(&h->bulk, g, 0);
+                if (g) cudaGraphDestroy(g);
+                h->launches = l0;
+                if (e != cudaSuccess) {      // no graph on this stream: stay eager
+                    cudaGetLastError();
+                    h->bulk = nullptr;
+                    h->bulk_off = true;
+                }
+            }
+            if (h->bulk) {
+                const int per = h->split1d ? 2 : (h->p.dim == 2 ? 2 : 4);
+                while (nsteps - tail - s >= kBulkSteps) {
+                    CK(cudaGraphLaunch(h->bulk, h->st));
+                    h->launches += (long long)per * kBulkSteps;
+                    s += kBulkSteps;
+                }
+            }
+        }
+    }
+    for (; s < nsteps; ++s) {
         void* sn = nullptr;
         if (snap && s == nsteps - 1) sn = h->psi;
         if (snap && s == nsteps - 2) sn = h->prev;
-        DISPATCH(h, launch_row, h, ROW_FULL, sn);
+        launch_step(sn);
         if (snap && s == nsteps - 2) {
             CK(cudaMemcpyAsync(h->info_prev, h->info, INFO_LEN * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
             h->prev_valid = true;
@@ -1107,6 +1152,7 @@ int fgpe_apply_op(fgpe_t* h, int op) {
 
 int fgpe_set_kernels(fgpe_t* h, int kernels) {
     if (!h) return fail(h, FGPE_E_ARG, "null handle");
+    if (h->bulk) { CK(cudaStreamSynchronize(h->st)); cudaGraphExecDestroy(h->bulk); h->bulk = nullptr; }
     const bool fast = kernels != FGPE_KERNELS_GENERIC;
     h->fast_row = fast && h->has_fast_row && kernels != FGPE_KERNELS_FAST_COL_ONLY;
     for (int a = 0; a < 3; ++a) h->fast_col[a] = fast && h->has_fast_col[a] && kernels != FGPE_KERNELS_FAST_ROW_ONLY;

@@ -42,7 +42,11 @@ enum {
 
 enum { FGPE_FP64 = 0, FGPE_FP32 = 1 };
 enum { FGPE_KERNELS_AUTO = 0, FGPE_KERNELS_GENERIC = 1,
-       FGPE_KERNELS_FAST_ROW_ONLY = 2, FGPE_KERNELS_FAST_COL_ONLY = 3 };
+       FGPE_KERNELS_FAST_ROW_ONLY = 2, FGPE_KERNELS_FAST_COL_ONLY = 3,
+       FGPE_KERNELS_SPLIT_1D = 4,  /* 1D: the two-pass N1 x N2 split even for
+                                      short lines */
+       FGPE_KERNELS_SINGLE_1D = 5  /* 1D: the single-block kernel whenever the
+                                      line fits one block (200 KB) */ };
 
 /* Step flags for fgpe_step_ex. */
 enum {

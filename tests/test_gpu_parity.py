@@ -185,3 +185,21 @@ def test_projection_branch(F, case):
     en_o, mu_o, mz_o = orc.energy()
     assert abs(mz_g - mag) < 1e-12 and abs(mz_o - mag) < 1e-12
     assert abs(en_g - en_o) <= 1e-10 * abs(en_o)
+
+
+@pytest.mark.parametrize("case", [(2, 2, 1, (64, 48)), (3, 1, 0, (16, 16, 12)), (1, 2, 1, (4096,))], ids=case_id)
+def test_bulk_graph_replay_is_bitwise_eager(F, case):
+    """Multi-step calls replay a captured graph of whole steps for their bulk;
+    with kernel profiling on the same steps run eagerly.  Same kernels, same
+    order: bitwise the same state, norms and CONV."""
+    p = case_params(case)
+    orc = O.Oracle(**oracle_kwargs(p))
+    phi = initial_state(orc, 4)
+    a, b = F.Propagator(**p), F.Propagator(**p)
+    a.set_state(phi); b.set_state(phi)
+    b.profile(True)
+    for n in (100, 37):
+        a.step(n); b.step(n)
+        assert np.array_equal(a.state(), b.state())
+        assert np.array_equal(a.normc(), b.normc())
+        assert a.conv() == b.conv()

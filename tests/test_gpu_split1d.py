@@ -12,7 +12,7 @@ pytestmark = pytest.mark.gpu
 
 CASES = [((1, 2, 1, (4096,)), "fp64", False), ((1, 2, 0, (4096,)), "fp64", False),
          ((1, 1, 1, (6000,)), "fp64", False), ((1, 1, 1, (4096,)), "fp64", True),
-         ((1, 2, 1, (8192,)), "fp32", False)]
+         ((1, 2, 1, (8192,)), "fp32", False), ((1, 2, 1, (2048,)), "fp64-split", False)]
 
 
 @pytest.fixture(scope="module")
@@ -37,7 +37,10 @@ def test_split_line_matches_oracle(F, case, precision, no_soc):
     orc.set_state(phi)
     if no_soc:
         orc.set_mag(mag)
-    prop = F.Propagator(**p, precision=precision, mag=mag)
+    kernels = "auto"
+    if precision.endswith("-split"):          # a line that fits one block, split on request
+        precision, kernels = precision[:-6], "split-1d"
+    prop = F.Propagator(**p, precision=precision, mag=mag, kernels=kernels)
     prop.set_state(phi)
     if case[2]:
         orc.normt(); prop.normt()
