@@ -187,6 +187,34 @@ def capture(args):
     a small case for ncu)."""
     import numpy as np
     import fortress_b200 as F
+    if args.workload == "fno":
+        # training steps of the learned-guess network (64^2, batch 64)
+        import torch
+        from fortress_b200 import fno as FN
+        net = FN.FNO(64, 64, seed=7)
+        a = FN.input_channels(np.random.default_rng(0).uniform(-1, 1, (64, 5)), 64)
+        tgt = torch.randn(6, 64 * 64 * 64, device="cuda", generator=torch.Generator("cuda").manual_seed(1))
+        net.forward(a)
+        for _ in range(args.warmup + args.steps):
+            net.forward(); net.loss(tgt); net.backward(); net.adam()
+        torch.cuda.synchronize()
+        assert not net.tc_error()
+        print(json.dumps({"capture": "fno-train-64x64-b64", "steps": args.warmup + args.steps,
+                          "loss": float(net.loss_dev.item())}))
+        return
+    if args.workload == "golden1d":
+        with open(os.path.join(ROOT, "tests", "golden", "fortress_1d_spin2.json")) as f:
+            golden = json.load(f)
+        cfg = F.RunConfig.from_text(golden["input1D"], 1)
+        prop = F.Propagator.from_config(cfg)
+        x = (-1.0 + 2.0 * np.arange(cfg.n[0]) / cfg.n[0]) * cfg.n[0] * cfg.d[0] / 2.0
+        prop.set_state(np.repeat(np.exp(-x * x / 2.0)[:, None], 5, axis=1).astype(np.complex128))
+        prop.normt()
+        prop.step(args.warmup + args.steps)
+        en, mu, mz, rms = prop.observables()
+        assert np.isfinite(en)
+        print(json.dumps({"capture": "golden-1d-spin2-2048", "steps": args.warmup + args.steps, "en": en}))
+        return
     if args.workload == "3d":
         from fortress_b200.config import RunConfig
         w = D3
@@ -239,9 +267,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--prep-steps", type=int, default=3000,
                     help="imaginary-time relaxation steps that build the initial state (untimed)")
-    ap.add_argument("--workload", default="q2d", choices=["q2d", "3d", "sweep"],
+    ap.add_argument("--workload", default="q2d", choices=["q2d", "3d", "sweep", "golden1d", "fno"],
                     help="q2d: 512^2 spin-2 real time (headline); 3d: 256^3 spin-1 imaginary time; "
-                         "sweep: 512 ragged q2D spin-1 instances in one batched graph launch")
+                         "sweep: 512 ragged q2D spin-1 instances in one batched graph launch; "
+                         "golden1d: the reference's published run (1D spin-2, 2048 points, to convergence); "
+                         "fno: with --capture only, learned-guess training steps")
     ap.add_argument("--capture", action="store_true",
                     help="run only the workload's step kernels (warmup + steps launches of each, on the "
                          "unrelaxed guess, no timing, no other work) for profiler captures")
@@ -249,6 +279,8 @@ def main():
     args.warmup = max(args.warmup, 3)
     if args.capture:
         return capture(args)
+    if args.workload == "fno" and not args.capture:
+        ap.error("--workload fno is a profiling case: use it with --capture")
     if args.workload != "q2d" and args.impl == "ours":
         return other_workload(args)
 
@@ -442,10 +474,56 @@ def gaussian_nd(p):
     return np.repeat(g[..., None], ms, axis=-1).astype(np.complex128)
 
 
+# Wall time of the reference's own published run (its OUTPUT/ folder): 1D
+# spin-2 SO-coupled imaginary time, NX=2048, run to CONV <= 1e-6.
+GOLDEN_REF_S = 653.739042
+
+
+def golden1d(args):
+    """The reference's published run through the library's driver loop: the
+    input records from the committed fixture, INITIALIZE's Gaussian, the
+    reference's stop rule; one line with the wall time to convergence."""
+    import numpy as np
+    import torch
+    import fortress_b200 as F
+    from fortress_b200.driver import run
+    with open(os.path.join(ROOT, "tests", "golden", "fortress_1d_spin2.json")) as f:
+        golden = json.load(f)
+    cfg = F.RunConfig.from_text(golden["input1D"], 1)
+    x = (-1.0 + 2.0 * np.arange(cfg.n[0]) / cfg.n[0]) * cfg.n[0] * cfg.d[0] / 2.0
+    g = np.sqrt(0.2) * np.exp(-cfg.alpha[0] * x * x / 2.0) / np.sqrt(np.sqrt(np.pi))
+    phi = np.repeat(g[:, None], 5, axis=1).astype(np.complex128)
+    clocks = ClockSampler(0)
+    prop = F.Propagator.from_config(cfg)
+    prop.set_state(phi)
+    res = run(prop, 4 * cfg.stp, cfg.stp, cfg.tol, cfg.dt, 1)       # warm-up: graphs, first launches
+    prop = F.Propagator.from_config(cfg)
+    prop.set_state(phi)
+    torch.cuda.synchronize()
+    clocks.start()
+    t0 = time.perf_counter()
+    res = run(prop, cfg.niter, cfg.stp, cfg.tol, cfg.dt, 1)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    clk = clocks.stop()
+    steps = res.final["ii_minus_1"] + 1
+    print(json.dumps({"metric": "wall time to convergence (reference's published run)", "value": wall,
+                      "unit": "s", "n_gpus": 1, "steps": steps, "warmup": 4 * cfg.stp,
+                      "ms_per_step": 1e3 * wall / steps, "higher_is_better": False, "scaling": "weak",
+                      "vs_baseline": wall / GOLDEN_REF_S, "dtype": "c128",
+                      "data": "the reference's INPUT/input1D.dat (committed fixture) and INITIALIZE's guess",
+                      "config": {"workload": "golden-1d-spin2-2048", "precision": "fp64",
+                                 "exit_iteration": res.final["ii_minus_1"], "converged": bool(res.final["exited"]),
+                                 "timing": "host wall clock around the driver loop (it syncs at every STP)"},
+                      "clocks": clk}))
+
+
 def other_workload(args):
     import numpy as np
     import torch
     import fortress_b200 as F
+    if args.workload == "golden1d":
+        return golden1d(args)
     from fortress_b200.config import RunConfig
     peak, peak_kind = measured_peaks()
     clocks = ClockSampler(0)

@@ -706,16 +706,18 @@ int fgpe_create(const fgpe_params* pin, fgpe_t** out) {
         h->k1.T = 512;
     }
     if (h->split1d) {
-        // row pass: R rows of n1 per block; column pass: TX columns of n2
+        // row pass: R rows of n1 per block; column pass: TX columns of n2.
+        // These lines are short and the passes latency-bound, so the tiles
+        // stay small enough for at least 128 blocks where the line allows.
         int R = 1;
-        for (int r = 1; r <= 64; r *= 2) {
-            if (h->n2 % r || (size_t)ms * r * padded_len(h->n1) * h->cs > budget) break;
+        for (int r = 2; r <= 64; r *= 2) {
+            if (h->n2 % r || h->n2 / r < 128 || (size_t)ms * r * padded_len(h->n1) * h->cs > budget) break;
             R = r;
             if ((size_t)ms * r * h->n1 >= 2048) break;
         }
         int TX = 1;
-        for (int tx = 1; tx <= 16; tx *= 2) {
-            if (h->n1 % tx || (size_t)ms * tx * padded_len(h->n2) * h->cs > budget) break;
+        for (int tx = 2; tx <= 16; tx *= 2) {
+            if (h->n1 % tx || h->n1 / tx < 128 || (size_t)ms * tx * padded_len(h->n2) * h->cs > budget) break;
             TX = tx;
             if ((size_t)tx * h->cs >= 32) break;
         }
