@@ -627,14 +627,15 @@ int fgpe_create(const fgpe_params* pin, fgpe_t** out) {
         }
     }
 
-    // 1D lines whose spinor needs more than 96 KB of shared memory: split
-    // N = n1*n2 (n1 the divisor nearest sqrt(N)) for the four-step transform.
-    // Above that size the single-block kernel (one SM) is the slower one: at
-    // 2048 spin-2 FP64 points a step takes 52 us there and 26-31 us split.
+    // 1D lines of N*M >= 3072 complex values (or too long for one block's
+    // shared memory) are split N = n1*n2 (n1 the divisor nearest sqrt(N)) for
+    // the four-step transform: from there on the two passes over many SMs beat
+    // the single-block kernel (FP64 step: spin-1 1024 points 16 vs 18 us,
+    // spin-2 2048 points 18 vs 53 us; at 512 points the single block wins).
     size_t off_tw1 = 0, off_tw2 = 0;
     const size_t line1d = (size_t)h->ms * padded_len(p.nx) * h->cs;
     const bool must_split = p.dim == 1 && line1d > 200 * 1024;
-    const bool prefer_split = p.dim == 1 && (line1d > 96 * 1024 || p.kernels == FGPE_KERNELS_SPLIT_1D) &&
+    const bool prefer_split = p.dim == 1 && ((long long)p.nx * h->ms >= 3072 || p.kernels == FGPE_KERNELS_SPLIT_1D) &&
                               p.kernels != FGPE_KERNELS_SINGLE_1D;
     if (must_split || prefer_split) {
         int best = 0;
