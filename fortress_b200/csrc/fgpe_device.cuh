@@ -154,6 +154,27 @@ template <typename T, bool INV> struct Dft<T, INV, 5> {
     }
 };
 
+// Twiddle powers w^1..w^(R-1) of w = tw[j]: in FP64 one table load and R-2
+// complex products (w^2k = (w^k)^2, w^(2k+1) = w^2k * w) instead of R-1 loads
+// that compete with the butterflies for the shared-memory/L1 bandwidth (the
+// row pass of the 512^2 spin-2 step: 50.6 -> 43.6 us); the products add a few
+// ulp.  In FP32 those ulp would be visible after a few steps, so FP32 loads
+// every power.  FGPE_TW_POW 0 loads them in FP64 too.
+#ifndef FGPE_TW_POW
+#define FGPE_TW_POW 1
+#endif
+template <typename T, int R>
+__device__ __forceinline__ void tw_powers(const cx<T>* __restrict__ tw, int j, int tstep, cx<T> (&w)[R]) {
+    if (!FGPE_TW_POW || sizeof(T) == 4) {
+#pragma unroll
+        for (int r = 1; r < R; ++r) w[r] = tw[j * r * tstep];
+        return;
+    }
+    w[1] = tw[j * tstep];
+#pragma unroll
+    for (int r = 2; r < R; ++r) w[r] = (r % 2 == 0) ? cmul(w[r / 2], w[r / 2]) : cmul(w[r - 1], w[1]);
+}
+
 template <typename T, bool INV, int R, class Map>
 __device__ __forceinline__ void fft_pass(cx<T>* s, const Map& mp, int nlines, int n, int Bp,
                                          const cx<T>* __restrict__ tw) {
@@ -172,13 +193,17 @@ __device__ __forceinline__ void fft_pass(cx<T>* s, const Map& mp, int nlines, in
         if (!INV) {
             Dft<T, false, R>::run(v);
             if (n2) {
+                cx<T> w[R];
+                tw_powers<T, R>(tw, n2, tstep, w);
 #pragma unroll
-                for (int r = 1; r < R; ++r) v[r] = cmul(v[r], tw[n2 * r * tstep]);
+                for (int r = 1; r < R; ++r) v[r] = cmul(v[r], w[r]);
             }
         } else {
             if (n2) {
+                cx<T> w[R];
+                tw_powers<T, R>(tw, n2, tstep, w);
 #pragma unroll
-                for (int r = 1; r < R; ++r) v[r] = cmulc(v[r], tw[n2 * r * tstep]);
+                for (int r = 1; r < R; ++r) v[r] = cmulc(v[r], w[r]);
             }
             Dft<T, true, R>::run(v);
         }
@@ -263,6 +288,24 @@ template <> struct A0<5> {
     }
 };
 
+// exp(-i CDT x) for |dt x| <= 1/16 by the Taylor series of sin/cos (real
+// time) or exp (imaginary time) truncated after the x^10 term: the first
+// omitted term is below (1/16)^11/11! ~ 8e-22, under FP64 rounding.
+template <typename T> __device__ __forceinline__ cx<T> small_phase(int imag, T th) {
+    const T t2 = th * th;
+    if (imag) {
+        // exp(-th) = sum (-th)^k/k!
+        const T e = (T)1 - th * ((T)1 - th * ((T)(1.0 / 2) - th * ((T)(1.0 / 6) - th * ((T)(1.0 / 24) - th * ((T)(1.0 / 120)
+                    - th * ((T)(1.0 / 720) - th * ((T)(1.0 / 5040) - th * ((T)(1.0 / 40320) - th * ((T)(1.0 / 362880)
+                    - th * (T)(1.0 / 3628800))))))))));
+        return mk<T>(e, (T)0);
+    }
+    const T cs = (T)1 - t2 * ((T)(1.0 / 2) - t2 * ((T)(1.0 / 24) - t2 * ((T)(1.0 / 720) - t2 * ((T)(1.0 / 40320)
+                 - t2 * (T)(1.0 / 3628800)))));
+    const T sn = th * ((T)1 - t2 * ((T)(1.0 / 6) - t2 * ((T)(1.0 / 120) - t2 * ((T)(1.0 / 5040) - t2 * (T)(1.0 / 362880)))));
+    return mk<T>(cs, -sn);
+}
+
 // v <- exp(-i CDT H_SO(k)) v with H_SO = A(beta) diag(L alpha) A(beta)^H,
 // alpha = 2 sqrt(gx^2 kx^2 + gy^2 ky^2) in 2D/3D (cgpe2d.f90:1571-1594) and
 // alpha = 2 gx kx, beta = 0 in 1D (cgpe1d.f90:1516-1520).
@@ -274,8 +317,15 @@ __device__ __forceinline__ void apply_soc(const StepConst& c, double kx, double 
         alpha = 2.0 * c.gx * kx;
     } else {
         const double ax = c.gx * kx, ay = c.gy * ky;
-        alpha = 2.0 * sqrt(ax * ax + ay * ay);
-        if (alpha > 1.0e-40) { cb = ax / (0.5 * alpha); sb = ay / (0.5 * alpha); }
+        const double r2 = ax * ax + ay * ay;
+        if (r2 > 0.0) {
+            // one reciprocal square root for |.|, cos beta and sin beta
+            const double ir = rsqrt(r2);
+            alpha = 2.0 * r2 * ir;
+            if (alpha > 1.0e-40) { cb = ax * ir; sb = ay * ir; }
+        } else {
+            alpha = 0.0;
+        }
     }
     if (alpha == 0.0) return;  // exp(0) = 1
     // phases e^{i c beta}, c = S-m: w_m = conj(P_m) v_m = e^{+i (S-m) beta} v_m
@@ -300,10 +350,13 @@ __device__ __forceinline__ void apply_soc(const StepConst& c, double kx, double 
         }
         u[r] = s;
     }
-    // u_L *= exp(-i CDT L alpha)
-    const cx<T> l1 = cdt_phase<T>(c.imag, (T)c.dt, (T)alpha);
+    // u_L *= exp(-i CDT L alpha); the angle dt*alpha is small for resolved
+    // grids, where the series of small_phase replaces sincos / exp
+    const T th = (T)(c.dt * alpha);
+    const bool small = fabs(th) <= (T)0.0625;
+    const cx<T> l1 = small ? small_phase<T>(c.imag, th) : cdt_phase<T>(c.imag, (T)c.dt, (T)alpha);
     // real time: exp(+i dt alpha) = conj; imaginary time: exp(+dt alpha)
-    const cx<T> lm1 = c.imag ? mk<T>(exp_t((T)(c.dt * alpha)), (T)0) : cconj(l1);
+    const cx<T> lm1 = c.imag ? (small ? small_phase<T>(1, -th) : mk<T>(exp_t(th), (T)0)) : cconj(l1);
 #pragma unroll
     for (int m = 0; m < MS; ++m) {
         const int L = m - S;
@@ -483,23 +536,6 @@ __device__ __forceinline__ void se_spin1(const StepConst& c, cx<T>* v) {
     v[2] = cadd(p3, cadd(cscale(u3, dc), w3));
 }
 
-// exp(-i CDT x) for |dt x| <= 1/16 by the Taylor series of sin/cos (real
-// time) or exp (imaginary time) truncated after the x^10 term: the first
-// omitted term is below (1/16)^11/11! ~ 8e-22, under FP64 rounding.
-template <typename T> __device__ __forceinline__ cx<T> small_phase(int imag, T th) {
-    const T t2 = th * th;
-    if (imag) {
-        // exp(-th) = sum (-th)^k/k!
-        const T e = (T)1 - th * ((T)1 - th * ((T)(1.0 / 2) - th * ((T)(1.0 / 6) - th * ((T)(1.0 / 24) - th * ((T)(1.0 / 120)
-                    - th * ((T)(1.0 / 720) - th * ((T)(1.0 / 5040) - th * ((T)(1.0 / 40320) - th * ((T)(1.0 / 362880)
-                    - th * (T)(1.0 / 3628800))))))))));
-        return mk<T>(e, (T)0);
-    }
-    const T cs = (T)1 - t2 * ((T)(1.0 / 2) - t2 * ((T)(1.0 / 24) - t2 * ((T)(1.0 / 720) - t2 * ((T)(1.0 / 40320)
-                 - t2 * (T)(1.0 / 3628800)))));
-    const T sn = th * ((T)1 - t2 * ((T)(1.0 / 6) - t2 * ((T)(1.0 / 120) - t2 * ((T)(1.0 / 5040) - t2 * (T)(1.0 / 362880)))));
-    return mk<T>(cs, -sn);
-}
 
 // exp(-i CDT V) at grid point (i, j, k): V = vx + vy + vz is separable, so
 // the factor is the product of the per-axis tables.

@@ -55,27 +55,6 @@ template <int N, int TX> struct ColTile {
     static __device__ __forceinline__ int at(int l, int e) { return ((l / TX) * LPN + e + (e >> 3)) * TX + (l % TX); }
 };
 
-// Twiddle powers w^1..w^(R-1) of w = tw[j]: in FP64 one table load and R-2
-// complex products (w^2k = (w^k)^2, w^(2k+1) = w^2k * w) instead of R-1 loads
-// that compete with the butterflies for the shared-memory/L1 bandwidth (the
-// row pass of the 512^2 spin-2 step: 50.6 -> 43.6 us); the products add a few
-// ulp.  In FP32 those ulp would be visible after a few steps, so FP32 loads
-// every power.  FGPE_TW_POW 0 loads them in FP64 too.
-#ifndef FGPE_TW_POW
-#define FGPE_TW_POW 1
-#endif
-template <typename T, int R>
-__device__ __forceinline__ void tw_powers(const cx<T>* __restrict__ tw, int j, int tstep, cx<T> (&w)[R]) {
-    if (!FGPE_TW_POW || sizeof(T) == 4) {
-#pragma unroll
-        for (int r = 1; r < R; ++r) w[r] = tw[j * r * tstep];
-        return;
-    }
-    w[1] = tw[j * tstep];
-#pragma unroll
-    for (int r = 2; r < R; ++r) w[r] = (r % 2 == 0) ? cmul(w[r / 2], w[r / 2]) : cmul(w[r - 1], w[1]);
-}
-
 // One radix-R pass over NL lines.  Between two passes only the threads that
 // share lines need to wait for each other: when every thread has exactly one
 // task in this pass and in the next (same radix, so the same task -> line
