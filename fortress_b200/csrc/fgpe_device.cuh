@@ -431,6 +431,11 @@ __device__ __forceinline__ void hmul(const cx<T>* c, const cx<T>* v, cx<T>* y) {
     y[4] = cadd(cmulc(v[2], c[4]), cmulc(v[3], c[5]));
 }
 
+// 1/k for k <= 41 (k = 0 unused), so that the Taylor loops of the spin-2 SE
+// multiply instead of dividing (an FP64 division costs tens of instructions).
+__constant__ double kInvK[42] = {0.0, 1.0 / 1, 1.0 / 2, 1.0 / 3, 1.0 / 4, 1.0 / 5, 1.0 / 6, 1.0 / 7, 1.0 / 8, 1.0 / 9, 1.0 / 10, 1.0 / 11, 1.0 / 12, 1.0 / 13, 1.0 / 14, 1.0 / 15, 1.0 / 16, 1.0 / 17, 1.0 / 18, 1.0 / 19, 1.0 / 20, 1.0 / 21, 1.0 / 22, 1.0 / 23, 1.0 / 24, 1.0 / 25, 1.0 / 26, 1.0 / 27, 1.0 / 28, 1.0 / 29, 1.0 / 30, 1.0 / 31, 1.0 / 32, 1.0 / 33, 1.0 / 34, 1.0 / 35, 1.0 / 36, 1.0 / 37, 1.0 / 38, 1.0 / 39, 1.0 / 40, 1.0 / 41};
+template <typename T> __device__ __forceinline__ T inv_k(int k) { return (T)kInvK[k]; }
+
 template <typename T> struct Eps;
 template <> struct Eps<double> { static __device__ __forceinline__ double v() { return 1.1e-16; } };
 template <> struct Eps<float> { static __device__ __forceinline__ float v() { return 6.0e-8f; } };
@@ -465,10 +470,13 @@ __device__ __forceinline__ void se_spin2(const StepConst& c, cx<T>* v) {
     const T nrm = dt * col;
     if (nrm == (T)0) return;
     int nsub = 1;
-    if (nrm > (T)0.5) nsub = (int)ceil(nrm / (T)0.5);
-    if (nsub > 4096) nsub = 4096;
-    const T h = dt / (T)nsub;  // z = -i h (real) or -h (imag)
-    const T hn = nrm / (T)nsub;
+    T h = dt, hn = nrm;        // z = -i h (real) or -h (imag)
+    if (nrm > (T)0.5) {
+        nsub = (int)ceil(nrm / (T)0.5);
+        if (nsub > 4096) nsub = 4096;
+        h = dt / (T)nsub;
+        hn = nrm / (T)nsub;
+    }
     // Number of Taylor terms fixed beforehand: the remainder after K terms is
     // below hn^(K+1)/(K+1)! * e^hn relative to |v|, and |y| >= e^-hn |v|
     // (e^{-h H} can contract by at most e^-hn), so stop once
@@ -479,7 +487,7 @@ __device__ __forceinline__ void se_spin2(const StepConst& c, cx<T>* v) {
     {
         const T e2 = (T)1 + (T)4 * hn;
         T bnd = hn * hn * (T)0.5;
-        while (bnd * e2 > Eps<T>::v() * (T)0.5 && K < 40) { ++K; bnd *= hn / (T)(K + 1); }
+        while (bnd * e2 > Eps<T>::v() * (T)0.5 && K < 40) { ++K; bnd *= hn * inv_k<T>(K + 1); }
     }
     for (int sidx = 0; sidx < nsub; ++sidx) {
         cx<T> term[5], y[5];
@@ -487,7 +495,7 @@ __device__ __forceinline__ void se_spin2(const StepConst& c, cx<T>* v) {
         for (int m = 0; m < 5; ++m) { term[m] = v[m]; y[m] = v[m]; }
         for (int k = 1; k <= K; ++k) {
             hmul<T>(ca, term, hv);
-            const T f = h / (T)k;
+            const T f = h * inv_k<T>(k);
 #pragma unroll
             for (int m = 0; m < 5; ++m) {
                 if (c.imag) term[m] = mk<T>(-f * hv[m].x, -f * hv[m].y);
@@ -511,18 +519,34 @@ __device__ __forceinline__ void se_spin1(const StepConst& c, cx<T>* v) {
     cx<T> B1 = cscale(cmulc(v[1], v[0]), t1);
     const T aa = cabs2(A1), bb = cabs2(B1);
     const T r2 = aa + bb;
-    const T r = sqrt_t(r2);
     const T dt = (T)c.dt;
-    const T x = dt * r;   // |OMEGA|
-    const bool big = c.se_ge ? (x >= (T)1e-40) : (x > (T)1e-40);
     T dc;                 // DELTA*CDT^2 (real)
     cx<T> kc;             // KAPPA*CDT
+    const T z = dt * dt * r2;   // |OMEGA|^2
+    if (z <= (T)(1.0 / 256)) {
+        // |OMEGA| <= 1/16: 2 sinh^2(x/2)/x^2 = sum x^2n/(2n+2)!, sinh(x)/x =
+        // sum x^2n/(2n+1)! (sin: x^2 -> -x^2), to x^10 (next term < 1e-20
+        // relative): no square root, division or transcendental call, and the
+        // |OMEGA| -> 0 limits (DELTA*CDT^2 = CDT^2/2, KAPPA*CDT = -i CDT) are
+        // the leading terms
+        const T zz = c.imag ? z : -z;
+        const T g = (T)(1.0 / 2) + zz * ((T)(1.0 / 24) + zz * ((T)(1.0 / 720) + zz * ((T)(1.0 / 40320) +
+                    zz * ((T)(1.0 / 3628800) + zz * (T)(1.0 / 479001600)))));
+        const T f = (T)1 + zz * ((T)(1.0 / 6) + zz * ((T)(1.0 / 120) + zz * ((T)(1.0 / 5040) +
+                    zz * ((T)(1.0 / 362880) + zz * (T)(1.0 / 39916800)))));
+        dc = (c.imag ? (T)1 : (T)-1) * dt * dt * g;
+        kc = c.imag ? mk<T>(-dt * f, 0) : mk<T>(0, -dt * f);
+    } else {
+    const T r = sqrt_t(r2);
+    const T x = dt * r;   // |OMEGA|
+    const bool big = c.se_ge ? (x >= (T)1e-40) : (x > (T)1e-40);
     if (c.imag) {
         if (big) { T sh = sinh_t((T)0.5 * x); dc = (T)2 * sh * sh / r2; kc = mk<T>(-sinh_t(x) / r, 0); }
         else { dc = (T)0.5 * dt * dt; kc = mk<T>(-dt, 0); }
     } else {
         if (big) { T sn = sin_t((T)0.5 * x); dc = (T)-2 * sn * sn / r2; kc = mk<T>(0, -sin_t(x) / r); }
         else { dc = (T)-0.5 * dt * dt; kc = mk<T>(0, -dt); }
+    }
     }
     const cx<T> p1 = v[0], p2 = v[1], p3 = v[2];
     // TMP(1) = dc (|A1|^2 p1 + A1 B1* p3) + kc A1 p2
