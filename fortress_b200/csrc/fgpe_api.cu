@@ -1165,7 +1165,36 @@ int fgpe_set_kernels(fgpe_t* h, int kernels) {
 int fgpe_norms_async(fgpe_t* h, double* dst) {
     if (!h || !dst) return fail(h, FGPE_E_ARG, "null argument");
     if (!h->norms_valid) return fail(h, FGPE_E_STATE, "no step taken since the state was set");
-    CK(cudaMemcpyAsync(dst, h->info + INFO_NORM, h->ms * sizeof(double), cudaMemcpyDefault, h->st));
+    // Device memory of this device and pinned host memory the device can
+    // address take a one-warp kernel in the step chain; anything else
+    // (pageable memory, another device) a copy.
+    cudaPointerAttributes at = {};
+    double* ddst = nullptr;
+    int cur = 0;
+    CK(cudaGetDevice(&cur));
+    if (cudaPointerGetAttributes(&at, dst) == cudaSuccess &&
+        ((at.type == cudaMemoryTypeHost && at.devicePointer) ||
+         (at.type == cudaMemoryTypeDevice && at.device == cur)))
+        ddst = (double*)at.devicePointer;
+    else
+        cudaGetLastError();
+    if (!ddst) {
+        CK(cudaMemcpyAsync(dst, h->info + INFO_NORM, h->ms * sizeof(double), cudaMemcpyDefault, h->st));
+        return FGPE_OK;
+    }
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CK(cudaStreamIsCapturing(h->st, &cs));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(1);
+    cfg.blockDim = dim3(32);
+    cfg.stream = h->st;
+    cudaLaunchAttribute la[1];
+    la[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    la[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = la;
+    cfg.numAttrs = cs == cudaStreamCaptureStatusNone ? 1 : 0;
+    CK(cudaLaunchKernelEx(&cfg, k_norms_out, (const double*)h->info, ddst, h->ms));
+    h->launches++;
     return FGPE_OK;
 }
 

@@ -679,6 +679,15 @@ __global__ void k_apply_scale(T* psi, long long n2, long long per2, double* info
         psi[t] = (T)(info[INFO_SC + t / per2] * (double)psi[t]);
 }
 
+// Per-step read-back of NORMC: copies the MS component norms to dst, which is
+// device memory or pinned host memory that the device addresses directly.  As
+// a programmatic dependent launch it waits for the step's last pass and keeps
+// the step chain on the SMs instead of a copy-engine transfer between steps.
+__global__ void k_norms_out(const double* __restrict__ info, double* __restrict__ dst, int ms) {
+    asm volatile("griddepcontrol.wait;\n" ::: "memory");
+    if ((int)threadIdx.x < ms) dst[threadIdx.x] = info[INFO_NORM + threadIdx.x];
+}
+
 // Unfused single operators on a full real/Fourier-space buffer (parity
 // checks of individual reference subroutines).
 template <typename T, int MS>
