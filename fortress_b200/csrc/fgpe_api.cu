@@ -184,12 +184,19 @@ template <typename T, int MS, int N> constexpr int row_th() {
 template <typename T, int MS, int N> constexpr int col_th() {
     return FGPE_COL_TH ? FGPE_COL_TH : fast_threads(MS * col_tx<T>() * N / 8);
 }
-// Wide column tiles: 128 contiguous bytes of x per line element (8 complex
-// doubles, 16 complex floats), for grids with enough tiles (3D) where the
-// 32-byte segments of the narrow tiles waste DRAM bursts.
-template <typename T> constexpr int col_txw() { return 128 / (int)sizeof(cx<T>); }
+// Wide column tiles: FGPE_COL_WIDE_BYTES (default 128) contiguous bytes of x
+// per line element (8 complex doubles, 16 complex floats), for grids with
+// enough tiles (3D) where the 32-byte segments of the narrow tiles waste DRAM
+// bursts; FGPE_COL_NBUF_W shared buffers per block (default FGPE_COL_NBUF).
+#ifndef FGPE_COL_WIDE_BYTES
+#define FGPE_COL_WIDE_BYTES 128
+#endif
+#ifndef FGPE_COL_NBUF_W
+#define FGPE_COL_NBUF_W FGPE_COL_NBUF
+#endif
+template <typename T> constexpr int col_txw() { return FGPE_COL_WIDE_BYTES / (int)sizeof(cx<T>); }
 template <typename T, int MS, int N> constexpr size_t col_smem_w() {
-    return (size_t)FGPE_COL_NBUF * MS * cpad(N) * col_txw<T>() * sizeof(cx<T>);
+    return (size_t)FGPE_COL_NBUF_W * MS * cpad(N) * col_txw<T>() * sizeof(cx<T>);
 }
 template <typename T, int MS, int N> constexpr bool wide_ok() { return col_smem_w<T, MS, N>() <= 113 * 1024; }
 template <typename T, int MS, int N> constexpr int col_th_w() { return fast_threads(MS * col_txw<T>() * N / 8); }
@@ -223,7 +230,7 @@ template <typename T, int MS, int N> int setup_fast_col(fgpe_t* h, int n_other, 
     if constexpr (wide_ok<T, MS, N>()) {
         if (h->p.nx % col_txw<T>() == 0) {
             const int ntw = (h->p.nx / col_txw<T>()) * n_other;
-            const int g = grid_for(k_col_fast<T, MS, N, col_txw<T>(), col_th_w<T, MS, N>()>, col_th_w<T, MS, N>(),
+            const int g = grid_for(k_col_fast<T, MS, N, col_txw<T>(), col_th_w<T, MS, N>(), FGPE_COL_NBUF_W>, col_th_w<T, MS, N>(),
                                    col_smem_w<T, MS, N>(), ntw);
             if (g > 0 && ntw >= 4 * g) { *wide = true; return g; }
         }
@@ -264,7 +271,7 @@ template <typename T, int MS, int N> void run_fast_row(fgpe_t* h, const RowArgs&
 template <typename T, int MS, int N> void run_fast_col(fgpe_t* h, int axis, const ColArgs& a) {
     if constexpr (wide_ok<T, MS, N>()) {
         if (h->col_wide[axis]) {
-            launch_pdl(h, k_col_fast<T, MS, N, col_txw<T>(), col_th_w<T, MS, N>()>, h->fast_col_grid[axis],
+            launch_pdl(h, k_col_fast<T, MS, N, col_txw<T>(), col_th_w<T, MS, N>(), FGPE_COL_NBUF_W>, h->fast_col_grid[axis],
                        col_th_w<T, MS, N>(), col_smem_w<T, MS, N>(), a);
             return;
         }

@@ -26,6 +26,13 @@ template <typename C> __host__ __device__ __forceinline__ C cmul(C a, C b) {
 template <typename C> __host__ __device__ __forceinline__ C cmulc(C a, C b) {
     C r; r.x = a.x * b.x + a.y * b.y; r.y = a.y * b.x - a.x * b.y; return r;
 }
+// acc + a * b and acc + a * conj(b), each part one chain of two FMAs onto acc
+template <typename C> __host__ __device__ __forceinline__ C cmac(C acc, C a, C b) {
+    C r; r.x = fma(a.x, b.x, fma(-a.y, b.y, acc.x)); r.y = fma(a.x, b.y, fma(a.y, b.x, acc.y)); return r;
+}
+template <typename C> __host__ __device__ __forceinline__ C cmacc(C acc, C a, C b) {
+    C r; r.x = fma(a.x, b.x, fma(a.y, b.y, acc.x)); r.y = fma(a.y, b.x, fma(-a.x, b.y, acc.y)); return r;
+}
 template <typename C> __host__ __device__ __forceinline__ C cconj(C a) { a.y = -a.y; return a; }
 template <typename C, typename S> __host__ __device__ __forceinline__ C cscale(C a, S s) { a.x *= s; a.y *= s; return a; }
 // multiply by i (sign = +1) or -i (sign = -1)
@@ -421,14 +428,15 @@ __device__ __forceinline__ void couplings2(const cx<T>* v, T t1, T t2, cx<T>* c)
     p = cmulc(v[0], v[1]); c[5] = mk<T>(t1 * fm.x - a * p.x, t1 * fm.y - a * p.y);
 }
 
-// y = H v for the zero-diagonal Hermitian H with upper entries c.
+// y = H v for the zero-diagonal Hermitian H with upper entries c; every
+// further product of a row accumulates by FMA onto the first one.
 template <typename T>
 __device__ __forceinline__ void hmul(const cx<T>* c, const cx<T>* v, cx<T>* y) {
-    y[0] = cadd(cmul(c[0], v[1]), cmul(c[1], v[2]));
-    y[1] = cadd(cmulc(v[0], c[0]), cmul(c[2], v[2]));
-    y[2] = cadd(cadd(cmulc(v[0], c[1]), cmulc(v[1], c[2])), cadd(cmul(c[3], v[3]), cmul(c[4], v[4])));
-    y[3] = cadd(cmulc(v[2], c[3]), cmul(c[5], v[4]));
-    y[4] = cadd(cmulc(v[2], c[4]), cmulc(v[3], c[5]));
+    y[0] = cmac(cmul(c[0], v[1]), c[1], v[2]);
+    y[1] = cmac(cmulc(v[0], c[0]), c[2], v[2]);
+    y[2] = cmac(cmac(cmacc(cmulc(v[0], c[1]), v[1], c[2]), c[3], v[3]), c[4], v[4]);
+    y[3] = cmac(cmulc(v[2], c[3]), c[5], v[4]);
+    y[4] = cmacc(cmulc(v[2], c[4]), v[3], c[5]);
 }
 
 // 1/k for k <= 41 (k = 0 unused), so that the Taylor loops of the spin-2 SE

@@ -361,10 +361,14 @@ __global__ void __launch_bounds__(TH, FGPE_COL_MINB) k_col_fast(StepConst c, Col
         // (the transform is linear); otherwise it takes its own sweep
         const bool fold = (a.flags & COL_SCALE) && (a.flags & COL_KOP);
         if ((a.flags & COL_SCALE) && !fold) {
-            for (int idx = threadIdx.x; idx < MS * N * TX; idx += TH) {
-                const int t = idx % TX, q = idx / TX, e = q % N, m = q / N;
-                cx<T>& v = cur[(m * LPN + e + (e >> 3)) * TX + t];
-                v = cscale(v, fac[m]);
+            // component loop outermost and unrolled: fac[] stays in registers
+#pragma unroll
+            for (int m = 0; m < MS; ++m) {
+                for (int idx = threadIdx.x; idx < N * TX; idx += TH) {
+                    const int t = idx % TX, e = idx / TX;
+                    cx<T>& v = cur[(m * LPN + e + (e >> 3)) * TX + t];
+                    v = cscale(v, fac[m]);
+                }
             }
             __syncthreads();
         }

@@ -135,8 +135,10 @@ enum { FGPE_OP_FFT = 1, FGPE_OP_KE = 2, FGPE_OP_SOC = 3, FGPE_OP_BFT = 4,
 int fgpe_apply_op(fgpe_t *h, int op);
 
 /* Non-blocking variant of fgpe_norms: enqueues the copy of the last step's
- * NORMC (M doubles) into dst, which must be pinned host memory (or device
- * memory) and is valid after the handle's stream has been synchronised. */
+ * NORMC (M doubles) into dst, valid after the handle's stream has been
+ * synchronised.  Pinned host memory and device memory of the handle's device
+ * are written by a one-warp kernel in the step chain (no copy-engine
+ * transfer between steps); other memory takes an asynchronous copy. */
 int fgpe_norms_async(fgpe_t *h, double *dst);
 
 /* Kernel timing with CUDA events recorded on the handle's stream around
