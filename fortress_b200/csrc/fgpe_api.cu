@@ -61,6 +61,9 @@ struct fgpe_s {
     int n1 = 0, n2 = 0;
     Launch r1d, c1d;
     const void *twn = nullptr, *tw1 = nullptr, *tw2 = nullptr;
+    // the same split on one thread-block cluster for a whole call (k_cl1d)
+    bool cl1d = false;
+    size_t cl1d_smem = 0;
     // CUDA graph of kBulkSteps whole steps without snapshots, replayed for
     // the bulk of multi-step calls (built on first use, dropped when the
     // kernel choice changes)
@@ -147,6 +150,7 @@ template <typename T, int MS> cudaError_t set_smem_attrs() {
     if (e == cudaSuccess) e = allow_smem(k_1d<T, MS>);
     if (e == cudaSuccess) e = allow_smem(k_r1d<T, MS>);
     if (e == cudaSuccess) e = allow_smem(k_c1d<T, MS>);
+    if (e == cudaSuccess) e = allow_smem(k_cl1d<T, MS>);
     return e;
 }
 
@@ -414,6 +418,48 @@ void launch_c1d(fgpe_t* h, int mode, void* snap) {
     h->launches++;
 }
 
+// The cluster form of the 1D split when n1 and n2 divide over the cluster,
+// both halves of Q fit the CTAs' shared memory and the cluster can be
+// resident; otherwise h->cl1d stays false and the two passes run.
+template <typename T, int MS>
+void setup_cl1d(fgpe_t* h) {
+    h->cl1d = false;
+    if (h->n1 % CL1D || h->n2 % CL1D) return;
+    const size_t smem = (size_t)MS * ((size_t)(h->n2 / CL1D) * padded_len(h->n1) +
+                                      (size_t)padded_len(h->n2) * (h->n1 / CL1D)) * sizeof(cx<T>);
+    if (smem > 200 * 1024) return;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(CL1D);
+    cfg.blockDim = dim3(256);
+    cfg.dynamicSmemBytes = smem;
+    int nc = 0;
+    if (cudaOccupancyMaxActiveClusters(&nc, k_cl1d<T, MS>, &cfg) != cudaSuccess || nc < 1) {
+        cudaGetLastError();
+        return;
+    }
+    h->cl1d = true;
+    h->cl1d_smem = smem;
+}
+
+// All nsteps of a call in one launch of the cluster kernel.
+template <typename T, int MS>
+void launch_cl1d(fgpe_t* h, int nsteps, void* snap_last, void* snap_prev) {
+    Cluster1dArgs a;
+    a.S = h->S; a.snap_last = snap_last; a.snap_prev = snap_prev;
+    a.twn = h->twn; a.tw1 = h->tw1; a.tw2 = h->tw2;
+    a.info = h->info; a.info_prev = h->info_prev;
+    a.n1 = h->n1; a.n2 = h->n2; a.nsteps = nsteps;
+    ProfScope ps(h, 3);
+    k_cl1d<T, MS><<<CL1D, 256, h->cl1d_smem, h->st>>>(h->sc, a);
+    h->launches++;
+}
+
+// Kernel launches of one step call of k whole steps on h.
+static long long step_launches(const fgpe_t* h, int k) {
+    if (h->cl1d) return 1;
+    return (long long)k * (h->p.dim == 1 ? (h->split1d ? 2 : 1) : (h->p.dim == 2 ? 2 : 4));
+}
+
 // dispatch on (precision, spin)
 #define DISPATCH(h, FN, ...)                                                  \
     do {                                                                      \
@@ -642,7 +688,9 @@ int fgpe_create(const fgpe_params* pin, fgpe_t** out) {
     size_t off_tw1 = 0, off_tw2 = 0;
     const size_t line1d = (size_t)h->ms * padded_len(p.nx) * h->cs;
     const bool must_split = p.dim == 1 && line1d > 200 * 1024;
-    const bool prefer_split = p.dim == 1 && ((long long)p.nx * h->ms >= 3072 || p.kernels == FGPE_KERNELS_SPLIT_1D) &&
+    const bool prefer_split = p.dim == 1 &&
+                              ((long long)p.nx * h->ms >= 3072 || p.kernels == FGPE_KERNELS_SPLIT_1D ||
+                               p.kernels == FGPE_KERNELS_CLUSTER_1D) &&
                               p.kernels != FGPE_KERNELS_SINGLE_1D;
     if (must_split || prefer_split) {
         int best = 0;
@@ -819,6 +867,19 @@ int fgpe_create(const fgpe_params* pin, fgpe_t** out) {
         CK(e1);
         CK(e2);
     }
+    // The cluster keeps a step on 8 SMs: it wins while the line is short
+    // (FP64 step, cluster vs two passes: spin-1 1024 points 11.6 vs 15.4 us,
+    // spin-2 2048 points 16.9 vs 18.3 us) and loses beyond (spin-2 4096
+    // points 28 vs 19 us), so by default it takes lines of N*M <= 10240.
+    const bool want_cl1d = p.kernels == FGPE_KERNELS_CLUSTER_1D ||
+                           (p.kernels != FGPE_KERNELS_SPLIT_1D && (long long)p.nx * h->ms <= 10240);
+    if (h->split1d && want_cl1d) {
+        DISPATCH(h, setup_cl1d, h);
+        if (!h->cl1d && p.kernels == FGPE_KERNELS_CLUSTER_1D) {
+            fgpe_destroy(h);
+            return fail(nullptr, FGPE_E_ARG, "1D split does not fit one 8-CTA cluster (N1, N2 multiples of 8, 200 KB)");
+        }
+    }
     CK(cudaGetLastError());
     *out = h;
     return FGPE_OK;
@@ -964,6 +1025,17 @@ int fgpe_step_ex(fgpe_t* h, int nsteps, int flags) {
         h->prev_valid = true;
     }
     h->psi_valid = false;
+    if (h->cl1d) {
+        // the whole call on one cluster: one launch, no graph
+        void* sl = snap ? h->psi : nullptr;
+        void* sp = (snap && nsteps >= 2) ? h->prev : nullptr;
+        DISPATCH(h, launch_cl1d, h, nsteps, sl, sp);
+        CK(cudaGetLastError());
+        if (sp) h->prev_valid = true;
+        h->psi_valid = snap;
+        h->norms_valid = true;
+        return FGPE_OK;
+    }
     // the passes of one step; sn: real-space snapshot target of the step
     auto launch_step = [&](void* sn) {
         if (h->split1d) {
@@ -1401,7 +1473,7 @@ int fgpe_batch_step(fgpe_batch_t* b, int nsteps) {
         }
         if (!b->exec || b->exec_steps != k) { int r = capture(b, k); if (r) return r; }
         BCK(cudaGraphLaunch(b->exec, b->origin));
-        for (fgpe_t* h : b->inst) h->launches += (long long)k * (h->p.dim == 1 ? (h->split1d ? 2 : 1) : (h->p.dim == 2 ? 2 : 4));
+        for (fgpe_t* h : b->inst) h->launches += step_launches(h, k);
         left -= k;
     }
     BCK(cudaStreamSynchronize(b->origin));
@@ -1428,7 +1500,7 @@ int fgpe_batch_step_timed(fgpe_batch_t* b, int nsteps, double* device_ms) {
         if (!b->exec || b->exec_steps != k) rc = capture(b, k);
         if (rc) break;
         err = cudaGraphLaunch(b->exec, b->origin);
-        for (fgpe_t* h : b->inst) h->launches += (long long)k * (h->p.dim == 1 ? (h->split1d ? 2 : 1) : (h->p.dim == 2 ? 2 : 4));
+        for (fgpe_t* h : b->inst) h->launches += step_launches(h, k);
         left -= k;
     }
     if (err == cudaSuccess && rc == FGPE_OK) err = cudaEventRecord(e1, b->origin);

@@ -12,8 +12,10 @@
 // The row pass's last block finishes the NORMC reduction in a fixed order and
 // publishes norms and the next scale (no host round trip).
 //   1D: the whole spinor lives in one block's shared memory and the block
-//       loops over steps.
+//       loops over steps; long lines take the four-step split, either as
+//       two passes per step or on one thread-block cluster for a whole call.
 #pragma once
+#include <cooperative_groups.h>
 #include "fgpe_device.cuh"
 #include "fgpe_kernels.h"
 
@@ -339,6 +341,160 @@ k_c1d(StepConst c, Split1dArgs a) {
     for (int idx = threadIdx.x; idx < nel; idx += blockDim.x) {
         const int t = idx % TX, q = idx / TX, e = q % n2, m = q / n2;
         S[(size_t)m * np + (size_t)e * n1 + x0 + t] = cmul(sm[(m * lpn + pad_idx(e)) * TX + t], twn[(size_t)(x0 + t) * c.fy[e]]);
+    }
+}
+
+// --------------------------------------- long 1D lines on one cluster
+// The row and column passes of k_r1d/k_c1d on one thread-block cluster of
+// CL1D CTAs that stays resident for all nsteps steps of a call.  Q (n2 rows
+// of n1 points per component) lives in the CTAs' shared memory: CTA r keeps
+// rows [r*RR, (r+1)*RR), RR = n2/CL1D, for the row phase, and transforms
+// columns [r*CC, (r+1)*CC), CC = n1/CL1D, in the column phase.  It gathers
+// those columns from the other CTAs' row tiles and scatters them back through
+// distributed shared memory, so a step touches no global memory except the
+// snapshots.  NORMC: each CTA's block sum goes to its slot in every CTA;
+// after the cluster barrier every CTA adds the CL1D sums in the same order and
+// derives the same scales (compute_scales is deterministic), so the scales need
+// no second exchange.  Per element the arithmetic is that of k_r1d/k_c1d; only
+// the order of the NORMC sum differs.  Three cluster barriers per step, taken
+// by every thread of every CTA on every step (no early exit).
+constexpr int CL1D = 8;
+
+template <typename T, int MS>
+__global__ void __cluster_dims__(CL1D, 1, 1) __launch_bounds__(256)
+k_cl1d(StepConst c, Cluster1dArgs a) {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
+    extern __shared__ __align__(16) unsigned char smraw[];
+    __shared__ double red[32 * (MS + 1)];
+    __shared__ double bsum[MS];
+    __shared__ double part[CL1D * MS];
+    __shared__ double s_sc[MS];
+    __shared__ double s_sig[2];
+    const int n1 = a.n1, n2 = a.n2;
+    const int RR = n2 / CL1D, CC = n1 / CL1D;
+    const int lp1 = padded_len(n1), lpn = padded_len(n2);
+    cx<T>* rows = (cx<T>*)smraw;                 // [m][r][pad(x)], r < RR
+    cx<T>* cols = rows + MS * RR * lp1;          // [m][pad(e)][t], t < CC
+    const RowMap rmp{lp1};
+    const ColMap cmp{CC, lpn};
+    const int rank = (int)cl.block_rank();
+    const int row0 = rank * RR, x0 = rank * CC;
+    const long long np = c.npts;
+    const cx<T>* twn = (const cx<T>*)a.twn;
+    const cx<T>* tw1 = (const cx<T>*)a.tw1;
+    const cx<T>* tw2 = (const cx<T>*)a.tw2;
+    cx<T>* S = (cx<T>*)a.S;
+    if (threadIdx.x < MS) s_sc[threadIdx.x] = a.info[INFO_SC + threadIdx.x];
+    if (threadIdx.x < 2) s_sig[threadIdx.x] = a.info[INFO_SIG + threadIdx.x];
+    __syncthreads();
+    // this CTA's rows, scaled by sc_m/N as the row pass loads them
+    const int nrow = MS * RR * n1;
+    for (int idx = threadIdx.x; idx < nrow; idx += blockDim.x) {
+        const int x = idx % n1, q = idx / n1, r = q % RR, m = q / RR;
+        rows[(m * RR + r) * lp1 + pad_idx(x)] =
+            cscale(S[(size_t)m * np + (size_t)(row0 + r) * n1 + x], (T)(s_sc[m] / (double)np));
+    }
+    __syncthreads();
+    const int ncol = MS * n2 * CC;
+    for (int step = 0; step < a.nsteps; ++step) {
+        // ---- row phase: F_N1, KE and SOC at k = k2 + N2*k1, F_N1^-1
+        block_fft<T, false>(rows, rmp, MS * RR, c.px, tw1);
+        for (int p = threadIdx.x; p < RR * n1; p += blockDim.x) {
+            const int x = p % n1, r = p / n1;
+            const int k = c.fy[row0 + r] + n2 * c.fx[x];
+            cx<T> v[MS];
+#pragma unroll
+            for (int m = 0; m < MS; ++m) v[m] = rows[(m * RR + r) * lp1 + pad_idx(x)];
+            apply_ke<T, MS>(c, k, 0, 0, v);
+            apply_soc<T, MS>(c, c.kx[k], 0.0, v);
+#pragma unroll
+            for (int m = 0; m < MS; ++m) rows[(m * RR + r) * lp1 + pad_idx(x)] = v[m];
+        }
+        __syncthreads();
+        block_fft<T, true>(rows, rmp, MS * RR, c.px, tw1);
+        cl.sync();                               // (1) every row tile is complete
+        // ---- column phase: gather with the conjugate twiddle, F_N2^-1,
+        // SE, SP, NORMC (+ snapshot), F_N2
+        for (int idx = threadIdx.x; idx < ncol; idx += blockDim.x) {
+            const int t = idx % CC, q = idx / CC, e = q % n2, m = q / n2;
+            const cx<T>* src = cl.map_shared_rank(rows, e / RR);
+            const cx<T> v = src[(m * RR + e % RR) * lp1 + pad_idx(x0 + t)];
+            cols[(m * lpn + pad_idx(e)) * CC + t] = cmulc(v, twn[(size_t)(x0 + t) * c.fy[e]]);
+        }
+        __syncthreads();
+        block_fft<T, true>(cols, cmp, MS * CC, c.py, tw2);
+        cx<T>* snap = step == a.nsteps - 1 ? (cx<T>*)a.snap_last
+                    : (step == a.nsteps - 2 ? (cx<T>*)a.snap_prev : nullptr);
+        double acc[MS];
+#pragma unroll
+        for (int m = 0; m < MS; ++m) acc[m] = 0.0;
+        for (int p = threadIdx.x; p < n2 * CC; p += blockDim.x) {
+            const int t = p % CC, e = p / CC;
+            const int x = x0 + t + n1 * e;             // 1D grid index
+            cx<T> v[MS];
+#pragma unroll
+            for (int m = 0; m < MS; ++m) v[m] = cols[(m * lpn + pad_idx(e)) * CC + t];
+            const cx<T> eV = pot_phase<T>(c, x, 0, 0);
+            apply_se<T, MS>(c, v);
+            apply_sp<T, MS>(c, eV, v);
+            const double w = c.wx[x];
+#pragma unroll
+            for (int m = 0; m < MS; ++m) {
+                acc[m] += w * ((double)v[m].x * (double)v[m].x + (double)v[m].y * (double)v[m].y);
+                cols[(m * lpn + pad_idx(e)) * CC + t] = v[m];
+            }
+            if (snap) {
+#pragma unroll
+                for (int m = 0; m < MS; ++m) snap[(size_t)m * np + x] = v[m];
+            }
+        }
+        block_sum<MS>(acc, red, bsum);
+        if (threadIdx.x < MS) {
+            for (int q = 0; q < CL1D; ++q) cl.map_shared_rank(part, q)[rank * MS + threadIdx.x] = bsum[threadIdx.x];
+        }
+        block_fft<T, false>(cols, cmp, MS * CC, c.py, tw2);
+        cl.sync();                               // (2) gathers done, block sums in place
+        if (threadIdx.x == 0) {
+            double n[MS], sc[MS], tot = 0;
+            for (int m = 0; m < MS; ++m) {
+                double s = 0;
+                for (int q = 0; q < CL1D; ++q) s += part[q * MS + m];
+                n[m] = s;
+                tot += s;
+            }
+            const int rc = compute_scales<MS>(c, n, s_sig, sc);
+            bool bad = !(tot == tot) || !(tot < 1e300);
+            for (int m = 0; m < MS; ++m) { s_sc[m] = sc[m]; bad = bad || !(sc[m] == sc[m]); }
+            if (rank == 0) {
+                double* info = a.info;
+                for (int m = 0; m < MS; ++m) { info[INFO_NORM + m] = n[m]; info[INFO_SC + m] = sc[m]; }
+                info[INFO_TOTAL] = tot;
+                info[INFO_SIG] = s_sig[0];
+                info[INFO_SIG + 1] = s_sig[1];
+                if (bad) info[INFO_ERR] = 1.0;
+                if (rc) info[INFO_ERR] = (double)rc;
+                if (step == a.nsteps - 2 && a.info_prev) {
+                    for (int i = 0; i < INFO_LEN; ++i) a.info_prev[i] = info[i];
+                }
+            }
+        }
+        __syncthreads();
+        // ---- scatter with the twiddle into the owners' rows, scaled for
+        // the next row phase (the last step leaves the scales pending)
+        const bool more = step + 1 < a.nsteps;
+        for (int idx = threadIdx.x; idx < ncol; idx += blockDim.x) {
+            const int t = idx % CC, q = idx / CC, e = q % n2, m = q / n2;
+            const cx<T> v = cmul(cols[(m * lpn + pad_idx(e)) * CC + t], twn[(size_t)(x0 + t) * c.fy[e]]);
+            cx<T>* dst = cl.map_shared_rank(rows, e / RR);
+            dst[(m * RR + e % RR) * lp1 + pad_idx(x0 + t)] = more ? cscale(v, (T)(s_sc[m] / (double)np)) : v;
+        }
+        cl.sync();                               // (3) rows complete for the next step
+    }
+    // Q back to global memory; the scales stay pending in info
+    for (int idx = threadIdx.x; idx < nrow; idx += blockDim.x) {
+        const int x = idx % n1, q = idx / n1, r = q % RR, m = q / RR;
+        S[(size_t)m * np + (size_t)(row0 + r) * n1 + x] = rows[(m * RR + r) * lp1 + pad_idx(x)];
     }
 }
 

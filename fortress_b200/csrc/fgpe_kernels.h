@@ -67,6 +67,20 @@ struct Split1dArgs {
     int mode;
 };
 
+// Long 1D lines on one thread-block cluster, resident for a whole call.
+struct Cluster1dArgs {
+    void* S;           // Q: loaded at entry, stored at exit (scales pending in info)
+    void* snap_last;   // real-space state after the last step, or null
+    void* snap_prev;   // real-space state after step nsteps-2, or null
+    const void* twn;   // W_N^j, j < N
+    const void* tw1;   // twiddles of the N1 transform
+    const void* tw2;   // twiddles of the N2 transform
+    double* info;      // INFO_* vector: scales and SIG in; norms, scales, SIG, error out
+    double* info_prev; // receives the INFO_* vector after step nsteps-2 (with snap_prev)
+    int n1, n2;
+    int nsteps;
+};
+
 struct OneDArgs {
     void* psi;
     void* snap_prev;

@@ -49,7 +49,7 @@ def make_params(dim, spin, n, d, dt, imag_time, tau, gamma=(0.0, 0.0, 0.0),
         p.gamma[i] = float(g[i])
         p.alpha[i] = float(alpha[i])
     p.precision = _abi.FGPE_FP32 if str(precision).lower() in ("fp32", "float32", "1") else _abi.FGPE_FP64
-    p.kernels = {"auto": 0, "generic": 1, "fast-row": 2, "fast-col": 3, "split-1d": 4, "single-1d": 5}[kernels]
+    p.kernels = {"auto": 0, "generic": 1, "fast-row": 2, "fast-col": 3, "split-1d": 4, "single-1d": 5, "cluster-1d": 6}[kernels]
     p.mag = float(mag)
     return p
 

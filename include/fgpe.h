@@ -43,10 +43,16 @@ enum {
 enum { FGPE_FP64 = 0, FGPE_FP32 = 1 };
 enum { FGPE_KERNELS_AUTO = 0, FGPE_KERNELS_GENERIC = 1,
        FGPE_KERNELS_FAST_ROW_ONLY = 2, FGPE_KERNELS_FAST_COL_ONLY = 3,
-       FGPE_KERNELS_SPLIT_1D = 4,  /* 1D: the two-pass N1 x N2 split even for
-                                      short lines */
-       FGPE_KERNELS_SINGLE_1D = 5  /* 1D: the single-block kernel whenever the
-                                      line fits one block (200 KB) */ };
+       FGPE_KERNELS_SPLIT_1D = 4,  /* 1D: the N1 x N2 split as two passes per
+                                      step, even for short lines */
+       FGPE_KERNELS_SINGLE_1D = 5, /* 1D: the single-block kernel whenever the
+                                      line fits one block (200 KB) */
+       FGPE_KERNELS_CLUSTER_1D = 6 /* 1D: the N1 x N2 split on one 8-CTA
+                                      thread-block cluster for a whole call,
+                                      even for short lines (N1 and N2 multiples
+                                      of 8; fgpe_create fails otherwise).  The
+                                      default for split lines of N*M <= 10240
+                                      when the cluster fits. */ };
 
 /* Step flags for fgpe_step_ex. */
 enum {
