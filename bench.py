@@ -90,6 +90,13 @@ def prepared_state(F, cfg_gs, prep_steps=3000):
 
 
 # ------------------------------------------------------------------ clocks
+def out_dir():
+    """Directory for the bench's side files (clock samples, autotune cache):
+    $FGPE_BENCH_OUT, else the system temporary directory."""
+    import tempfile
+    return os.environ.get("FGPE_BENCH_OUT") or tempfile.gettempdir()
+
+
 class ClockSampler:
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -98,7 +105,7 @@ class ClockSampler:
     def __init__(self, index=0):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{index}.csv")
+        self.path = os.path.join(out_dir(), f"clocks_rank{index}.csv")
 
     def start(self):
         try:
@@ -583,7 +590,7 @@ def other_workload(args):
     for i, p in enumerate(insts):
         b[i].set_state(gaussian_nd(p))
         b[i].normt()
-    tune = b.autotune(trial_steps=4, cache_path=os.path.join(ROOT, "gpurun_out", "autotune_cache.txt"))
+    tune = b.autotune(trial_steps=4, cache_path=os.path.join(out_dir(), "autotune_cache.txt"))
     npts = sum(int(np.prod(p["n"])) for p in insts)
     b.step(max(args.warmup, 4))
     clocks.start()

@@ -4,8 +4,8 @@
  *
  * TEST INFRASTRUCTURE ONLY.  This file is the oracle: only tests/, the smoke
  * check in __graft_entry__.py and the CPU-baseline legs of bench.py load it,
- * and only as the checker.  The product library (fortress_b200) never links,
- * loads or calls it.
+ * and only to compare results against.  The product library (fortress_b200)
+ * never links, loads or calls it.
  *
  * Every routine names the reference routine it restates (file:line in the
  * FORTRESS sources SRC/cgpe1d.f90, SRC/cgpe2d.f90, SRC/cgpe3d.f90,

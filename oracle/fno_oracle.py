@@ -1,5 +1,5 @@
 """FP64 numpy restatement of the Fourier neural operator used for the learned
-initial guess, forward and backward (test infrastructure only: the checker of
+initial guess, forward and backward (test infrastructure only: the oracle for
 the GPU kernels' values and gradients).
 
 Network (no reference counterpart; defined in fortress_b200/fno.py):

@@ -1,8 +1,8 @@
 """Python face of the CPU oracle (test infrastructure only).
 
 Only tests/, ``__graft_entry__.smoke()`` and the CPU-baseline legs of
-``bench.py`` import this module, and only as the checker.  The product package
-``fortress_b200`` never imports it.
+``bench.py`` import this module, and only to compare results against.  The
+product package ``fortress_b200`` never imports it.
 
 It wraps ``libcgpe_oracle.so`` (``cgpe_oracle.c``, the FP64 restatement of the
 FORTRESS operators) and restates, in Python, the reference's main loop
