@@ -38,7 +38,7 @@ EXPORTS = (
     "fgpe_batch_create", "fgpe_batch_destroy", "fgpe_batch_size", "fgpe_batch_instance",
     "fgpe_batch_last_error", "fgpe_batch_config", "fgpe_batch_step", "fgpe_batch_observables",
     "fgpe_batch_autotune", "fgpe_batch_tuning", "fgpe_set_kernels", "fgpe_normc_noalloc",
-    "fgpe_checkpoint_save", "fgpe_checkpoint_load", "fgpe_batch_step_timed",
+    "fgpe_checkpoint_save", "fgpe_checkpoint_load", "fgpe_batch_step_timed", "fgpe_norms_sink",
 )
 
 
@@ -91,6 +91,7 @@ def load():
         "fgpe_device_ok": ([], ip),
         "fgpe_kernel_launches": ([vp, ctypes.POINTER(ctypes.c_longlong)], ip),
         "fgpe_norms_async": ([vp, vp], ip),
+        "fgpe_norms_sink": ([vp, vp, ip], ip),
         "fgpe_profile_enable": ([vp, ip], ip),
         "fgpe_profile_read": ([vp, dp, ctypes.POINTER(ctypes.c_longlong), ip], ip),
         "fgpe_batch_create": ([ctypes.POINTER(Params), ip, ctypes.POINTER(vp)], ip),

@@ -1277,6 +1277,32 @@ int fgpe_norms_async(fgpe_t* h, double* dst) {
     return FGPE_OK;
 }
 
+int fgpe_norms_sink(fgpe_t* h, double* dst, int count) {
+    if (!h) return fail(h, FGPE_E_ARG, "null handle");
+    double* ddst = nullptr;
+    if (dst) {
+        if (count < 1) return fail(h, FGPE_E_ARG, "sink needs at least one record");
+        cudaPointerAttributes at = {};
+        int cur = 0;
+        CK(cudaGetDevice(&cur));
+        if (cudaPointerGetAttributes(&at, dst) == cudaSuccess &&
+            ((at.type == cudaMemoryTypeHost && at.devicePointer) ||
+             (at.type == cudaMemoryTypeDevice && at.device == cur)))
+            ddst = (double*)at.devicePointer;
+        cudaGetLastError();
+        if (!ddst) return fail(h, FGPE_E_ARG, "sink must be pinned host memory or memory of the handle's device");
+    }
+    // no step in flight may still write the previous ring
+    CK(cudaStreamSynchronize(h->st));
+    h->sc.sink = ddst;
+    h->sc.sink_n = ddst ? count : 0;
+    h->sc.sink_ctr = h->counters + 2;
+    CK(cudaMemsetAsync(h->counters + 2, 0, sizeof(unsigned), h->st));
+    // the bulk-step graph holds the kernel arguments it was captured with
+    if (h->bulk) { cudaGraphExecDestroy(h->bulk); h->bulk = nullptr; }
+    return FGPE_OK;
+}
+
 int fgpe_profile_enable(fgpe_t* h, int on) {
     if (!h) return fail(h, FGPE_E_ARG, "null handle");
     h->prof = on != 0;

@@ -269,7 +269,20 @@ struct StepConst {
     const void *pvx, *pvy, *pvz;    // potential factors exp(-i CDT ALPHA^2 X^2) per axis
     const int *fx, *fy, *fz;        // spectral position -> frequency index
     FftPlan px, py, pz;
+    double* sink;                   // per-step NORMC ring (pinned host or device), or null
+    unsigned* sink_ctr;             // steps appended since the ring was set
+    int sink_n;                     // records of MS doubles in the ring
 };
+
+// Append one step's NORMC to the sink ring (called by one thread).
+template <int MS>
+__device__ __forceinline__ void sink_norms(const StepConst& c, const double* n) {
+    if (!c.sink) return;
+    const unsigned k = *c.sink_ctr;
+    *c.sink_ctr = k + 1u;
+    double* d = c.sink + (size_t)(k % (unsigned)c.sink_n) * MS;
+    for (int m = 0; m < MS; ++m) d[m] = n[m];
+}
 
 // --------------------------------------------------------- SOC + KE at k
 // Spin-orbit eigenbasis at beta = 0 (cgpe1d.f90:627-675; the beta-dependent

@@ -83,6 +83,7 @@ __device__ __forceinline__ void finish_norms(const StepConst& c, const double* p
         double tot = 0, n[MS], sc[MS];
         for (int m = 0; m < MS; ++m) { n[m] = red[m]; tot += red[m]; info[INFO_NORM + m] = red[m]; }
         info[INFO_TOTAL] = tot;
+        sink_norms<MS>(c, n);
         const int rc = compute_scales<MS>(c, n, info + INFO_SIG, sc);
         bool bad = !(tot == tot) || !(tot < 1e300);
         for (int m = 0; m < MS; ++m) { info[INFO_SC + m] = sc[m]; bad = bad || !(sc[m] == sc[m]); }
@@ -470,6 +471,7 @@ k_cl1d(StepConst c, Cluster1dArgs a) {
                 double* info = a.info;
                 for (int m = 0; m < MS; ++m) { info[INFO_NORM + m] = n[m]; info[INFO_SC + m] = sc[m]; }
                 info[INFO_TOTAL] = tot;
+                sink_norms<MS>(c, n);
                 info[INFO_SIG] = s_sig[0];
                 info[INFO_SIG + 1] = s_sig[1];
                 if (bad) info[INFO_ERR] = 1.0;
@@ -555,6 +557,7 @@ k_1d(StepConst c, OneDArgs a) {
         if (threadIdx.x == 0) {
             double tot = 0, n[MS], sc[MS];
             for (int m = 0; m < MS; ++m) { n[m] = bsum[m]; tot += bsum[m]; }
+            sink_norms<MS>(c, n);
             const int rc = compute_scales<MS>(c, n, a.info + INFO_SIG, sc);
             for (int m = 0; m < MS; ++m) s_sc[m] = sc[m];
             if (rc) a.info[INFO_ERR] = (double)rc;

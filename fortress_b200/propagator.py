@@ -176,6 +176,11 @@ class Propagator:
         """Enqueue the last step's NORMC into pinned/device memory at ptr."""
         self._ck(self._L.fgpe_norms_async(self._h, ctypes.c_void_p(ptr)))
 
+    def norms_sink(self, ptr, count):
+        """From now on every step appends its NORMC to the ring of count
+        records at ptr (pinned host or device memory); ptr = 0 stops it."""
+        self._ck(self._L.fgpe_norms_sink(self._h, ctypes.c_void_p(ptr or None), int(count)))
+
     def profile(self, on=True):
         self._ck(self._L.fgpe_profile_enable(self._h, int(on)))
 

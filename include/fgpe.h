@@ -147,6 +147,15 @@ int fgpe_apply_op(fgpe_t *h, int op);
  * transfer between steps); other memory takes an asynchronous copy. */
 int fgpe_norms_async(fgpe_t *h, double *dst);
 
+/* Per-step NORMC without a call per step: after this call, every split step
+ * of the handle appends its NORMC (M doubles) to the ring dst[count][M], in
+ * step order, wrapping after count records; the step's own last block writes
+ * it (no extra kernel or copy).  dst is pinned host memory or memory of the
+ * handle's device, valid after the handle's stream has been synchronised; the
+ * record index restarts at 0 with each call.  dst = NULL stops it.  A batch
+ * graph captured before the call keeps the ring it was captured with. */
+int fgpe_norms_sink(fgpe_t *h, double *dst, int count);
+
 /* Kernel timing with CUDA events recorded on the handle's stream around
  * every kernel that fgpe_step launches.  fgpe_profile_read synchronises,
  * adds the elapsed times per kernel class -- [0] row pass (x), [1] column
