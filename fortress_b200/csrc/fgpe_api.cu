@@ -425,7 +425,7 @@ template <typename T, int MS>
 void setup_cl1d(fgpe_t* h) {
     h->cl1d = false;
     if (h->n1 % CL1D || h->n2 % CL1D) return;
-    const size_t smem = (size_t)MS * ((size_t)(h->n2 / CL1D) * padded_len(h->n1) +
+    const size_t smem = (size_t)MS * (2 * (size_t)(h->n2 / CL1D) * padded_len(h->n1) +
                                       (size_t)padded_len(h->n2) * (h->n1 / CL1D)) * sizeof(cx<T>);
     if (smem > 200 * 1024) return;
     cudaLaunchConfig_t cfg = {};
@@ -868,8 +868,8 @@ int fgpe_create(const fgpe_params* pin, fgpe_t** out) {
         CK(e2);
     }
     // The cluster keeps a step on 8 SMs: it wins while the line is short
-    // (FP64 step, cluster vs two passes: spin-1 1024 points 11.6 vs 15.4 us,
-    // spin-2 2048 points 16.9 vs 18.3 us) and loses beyond (spin-2 4096
+    // (FP64 step, cluster vs two passes: spin-1 1024 points 11.0 vs 15.4 us,
+    // spin-2 2048 points 16.7 vs 18.2 us) and loses beyond (spin-2 4096
     // points 28 vs 19 us), so by default it takes lines of N*M <= 10240.
     const bool want_cl1d = p.kernels == FGPE_KERNELS_CLUSTER_1D ||
                            (p.kernels != FGPE_KERNELS_SPLIT_1D && (long long)p.nx * h->ms <= 10240);

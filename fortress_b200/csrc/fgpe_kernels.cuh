@@ -353,12 +353,15 @@ k_c1d(StepConst c, Split1dArgs a) {
 // columns [r*CC, (r+1)*CC), CC = n1/CL1D, in the column phase.  It gathers
 // those columns from the other CTAs' row tiles and scatters them back through
 // distributed shared memory, so a step touches no global memory except the
-// snapshots.  NORMC: each CTA's block sum goes to its slot in every CTA;
-// after the cluster barrier every CTA adds the CL1D sums in the same order and
-// derives the same scales (compute_scales is deterministic), so the scales need
-// no second exchange.  Per element the arithmetic is that of k_r1d/k_c1d; only
-// the order of the NORMC sum differs.  Three cluster barriers per step, taken
-// by every thread of every CTA on every step (no early exit).
+// snapshots.  The row tiles alternate between two buffers: step s reads
+// buffer s&1 and scatters into buffer (s+1)&1, which nobody reads in step s,
+// so one cluster barrier after the row phase and one after the scatter are
+// all a step needs.  NORMC: each CTA's block sum goes to its slot in every
+// CTA; after the second barrier every CTA adds the CL1D sums in the same order
+// and derives the same scales (compute_scales is deterministic), and scales
+// its own rows for the next step.  Per element the arithmetic is that of
+// k_r1d/k_c1d; only the order of the NORMC sum differs.  Every thread of every
+// CTA takes both barriers on every step (no early exit).
 constexpr int CL1D = 8;
 
 template <typename T, int MS>
@@ -375,8 +378,10 @@ k_cl1d(StepConst c, Cluster1dArgs a) {
     const int n1 = a.n1, n2 = a.n2;
     const int RR = n2 / CL1D, CC = n1 / CL1D;
     const int lp1 = padded_len(n1), lpn = padded_len(n2);
-    cx<T>* rows = (cx<T>*)smraw;                 // [m][r][pad(x)], r < RR
-    cx<T>* cols = rows + MS * RR * lp1;          // [m][pad(e)][t], t < CC
+    const int nrow = MS * RR * n1;
+    const int rtile = MS * RR * lp1;               // one row buffer, [m][r][pad(x)]
+    cx<T>* rowbuf = (cx<T>*)smraw;                 // two row buffers
+    cx<T>* cols = rowbuf + 2 * rtile;              // [m][pad(e)][t], t < CC
     const RowMap rmp{lp1};
     const ColMap cmp{CC, lpn};
     const int rank = (int)cl.block_rank();
@@ -390,15 +395,16 @@ k_cl1d(StepConst c, Cluster1dArgs a) {
     if (threadIdx.x < 2) s_sig[threadIdx.x] = a.info[INFO_SIG + threadIdx.x];
     __syncthreads();
     // this CTA's rows, scaled by sc_m/N as the row pass loads them
-    const int nrow = MS * RR * n1;
     for (int idx = threadIdx.x; idx < nrow; idx += blockDim.x) {
         const int x = idx % n1, q = idx / n1, r = q % RR, m = q / RR;
-        rows[(m * RR + r) * lp1 + pad_idx(x)] =
+        rowbuf[(m * RR + r) * lp1 + pad_idx(x)] =
             cscale(S[(size_t)m * np + (size_t)(row0 + r) * n1 + x], (T)(s_sc[m] / (double)np));
     }
     __syncthreads();
     const int ncol = MS * n2 * CC;
     for (int step = 0; step < a.nsteps; ++step) {
+        cx<T>* rows = rowbuf + (step & 1) * rtile;        // this step's rows
+        cx<T>* next = rowbuf + ((step + 1) & 1) * rtile;  // scatter target
         // ---- row phase: F_N1, KE and SOC at k = k2 + N2*k1, F_N1^-1
         block_fft<T, false>(rows, rmp, MS * RR, c.px, tw1);
         for (int p = threadIdx.x; p < RR * n1; p += blockDim.x) {
@@ -414,7 +420,7 @@ k_cl1d(StepConst c, Cluster1dArgs a) {
         }
         __syncthreads();
         block_fft<T, true>(rows, rmp, MS * RR, c.px, tw1);
-        cl.sync();                               // (1) every row tile is complete
+        cl.sync();                               // (1) every row tile of this step is complete
         // ---- column phase: gather with the conjugate twiddle, F_N2^-1,
         // SE, SP, NORMC (+ snapshot), F_N2
         for (int idx = threadIdx.x; idx < ncol; idx += blockDim.x) {
@@ -455,7 +461,14 @@ k_cl1d(StepConst c, Cluster1dArgs a) {
             for (int q = 0; q < CL1D; ++q) cl.map_shared_rank(part, q)[rank * MS + threadIdx.x] = bsum[threadIdx.x];
         }
         block_fft<T, false>(cols, cmp, MS * CC, c.py, tw2);
-        cl.sync();                               // (2) gathers done, block sums in place
+        // ---- scatter with the twiddle into the owners' next rows
+        for (int idx = threadIdx.x; idx < ncol; idx += blockDim.x) {
+            const int t = idx % CC, q = idx / CC, e = q % n2, m = q / n2;
+            cx<T>* dst = cl.map_shared_rank(next, e / RR);
+            dst[(m * RR + e % RR) * lp1 + pad_idx(x0 + t)] =
+                cmul(cols[(m * lpn + pad_idx(e)) * CC + t], twn[(size_t)(x0 + t) * c.fy[e]]);
+        }
+        cl.sync();                               // (2) next rows complete, block sums in place
         if (threadIdx.x == 0) {
             double n[MS], sc[MS], tot = 0;
             for (int m = 0; m < MS; ++m) {
@@ -482,21 +495,22 @@ k_cl1d(StepConst c, Cluster1dArgs a) {
             }
         }
         __syncthreads();
-        // ---- scatter with the twiddle into the owners' rows, scaled for
-        // the next row phase (the last step leaves the scales pending)
-        const bool more = step + 1 < a.nsteps;
-        for (int idx = threadIdx.x; idx < ncol; idx += blockDim.x) {
-            const int t = idx % CC, q = idx / CC, e = q % n2, m = q / n2;
-            const cx<T> v = cmul(cols[(m * lpn + pad_idx(e)) * CC + t], twn[(size_t)(x0 + t) * c.fy[e]]);
-            cx<T>* dst = cl.map_shared_rank(rows, e / RR);
-            dst[(m * RR + e % RR) * lp1 + pad_idx(x0 + t)] = more ? cscale(v, (T)(s_sc[m] / (double)np)) : v;
+        // the next row phase loads its rows scaled by sc_m/N (the last step
+        // leaves the scales pending in info)
+        if (step + 1 < a.nsteps) {
+            for (int idx = threadIdx.x; idx < nrow; idx += blockDim.x) {
+                const int x = idx % n1, q = idx / n1, r = q % RR, m = q / RR;
+                cx<T>& v = next[(m * RR + r) * lp1 + pad_idx(x)];
+                v = cscale(v, (T)(s_sc[m] / (double)np));
+            }
+            __syncthreads();
         }
-        cl.sync();                               // (3) rows complete for the next step
     }
     // Q back to global memory; the scales stay pending in info
+    const cx<T>* fin = rowbuf + (a.nsteps & 1) * rtile;
     for (int idx = threadIdx.x; idx < nrow; idx += blockDim.x) {
         const int x = idx % n1, q = idx / n1, r = q % RR, m = q / RR;
-        S[(size_t)m * np + (size_t)(row0 + r) * n1 + x] = rows[(m * RR + r) * lp1 + pad_idx(x)];
+        S[(size_t)m * np + (size_t)(row0 + r) * n1 + x] = fin[(m * RR + r) * lp1 + pad_idx(x)];
     }
 }
 
