@@ -1,33 +1,40 @@
 #!/usr/bin/env python
 """Benchmark of the split-step spinor propagator on B200.
 
-Workload (the q2D configuration the headline metric is quoted on): spin-2
-SO-coupled real-time dynamics, NX=NY=512, DX=DY=0.05, DT=1e-4, Rb-87
-(mass 87, a0/a2/a4 = 87.93/91.28/99.18 a_B), NATOMS=50000, NUX=NUY=20 Hz,
-NUZ=500 Hz, ground state at GAMMAX=GAMMAY=1.0 quenched to GAMMAX=1.2.
-Synthetic initial state: the reference's default Gaussian guess relaxed by
-imaginary-time steps at gamma=(1,1) on the device, plus 1e-3 complex Gaussian
-noise (numpy PCG64 seed 2), renormalised (no dataset is involved).
+Default workload (the largest configuration, the one the time-to-ground-state
+target is stated on): 3D spin-1 SO-coupled imaginary-time propagation on a
+256^3 grid, DX=DY=DZ=0.1, DT=1e-3, Rb-87 (mass 87, a0/a2 = 101.8/100.4 a_B),
+NATOMS=100000, NUX=NUY=NUZ=50 Hz, GAMMAX=GAMMAY=GAMMAZ=0.5.  Synthetic
+initial state, identical in both arms: INITIALIZE's 3D spin-1 Gaussian
+(cgpe3d.f90:783-785) times (1 + 1e-3 u), u ~ U[0,1) from numpy PCG64 seed 3,
+then NORMT.  No dataset is involved.
 
-A step is one full Lie split step FFT->KE->SOC->BFT->SE->SP->NORMC of the
-whole 512^2 x 5 spinor.  Metric: grid-pt*steps/s (higher is better).
+A step is one full Lie split step FFT->KE->SOC->BFT->SE->SP->NORMC->NORMT of
+the whole 256^3 x 3 spinor.  Metric: grid-pt*steps/s (higher is better).
+The arithmetic is FP64 complex (the reference's precision); the FP32-bulk
+path (complex64 FFTs and exponentials, FP64 reductions) is reported beside it
+under "fp32".
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--precision fp64|fp32]
+                  [--workload 3d|q2d|sweep|golden1d]
 
-value : device time (CUDA events on the launching stream) of K steps, L2
-        flushed (256 MiB write) before every step, max over ranks.
-e2e   : the same K steps through the C ABI with host buffers: pinned H2D of
-        the state, every step's NORMC written by the step into a pinned host
-        ring (fgpe_norms_sink), D2H of the final state; device-timed with the
-        same flushes.
+value : device time (CUDA events on the launching stream) of K steps back to
+        back; the 805 MB state is larger than the 126 MB L2, so every step
+        streams it from HBM; max over ranks.
+e2e   : the same metric through the C ABI with host buffers, on a host wall
+        clock: pinned host->device upload of the state, K steps with every
+        step's NORMC written into a pinned host ring by the step itself
+        (fgpe_norms_sink), device->host download of the final state, and a
+        stream synchronisation, all inside the timed region.
 The reference arm (--impl reference) times the CPU restatement of the
-reference (oracle/, OpenMP on all host cores) on the same workload: the
-Fortran/FFTW/LAPACK reference cannot be compiled on this image.
+reference (oracle/, OpenMP on all host cores) on the same workload, the same
+initial state and the same config: the Fortran/FFTW/LAPACK reference cannot
+be compiled on this image.
 """
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -38,57 +45,64 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-WORKLOAD = dict(name="q2d-spin2-SO-realtime-512x512-quench", dim=2, spin=2, n=(512, 512),
-                d=(0.05, 0.05), dt=1e-4, mass=87.0, a=(87.93, 91.28, 99.18), natoms=50000,
-                nu=(20.0, 20.0, 500.0), gamma_gs=(1.0, 1.0), gamma=(1.2, 1.0))
 METRIC = "grid-pt*steps/s"
 
+# 3D spin-1 SO-coupled imaginary time (the largest configuration)
+D3 = dict(name="3d-spin1-SO-imag-256^3", dim=3, spin=1, n=(256, 256, 256), d=(0.1, 0.1, 0.1), dt=1e-3,
+          mass=87.0, a=(101.8, 100.4, 0.0), natoms=100000, nu=(50.0, 50.0, 50.0), gamma=(0.5, 0.5, 0.5),
+          switch_im=1, seed=3)
+# q2D spin-2 SO-coupled real-time quench (GAMMAX 1.0 -> 1.2 at t = 0)
+Q2D = dict(name="q2d-spin2-SO-realtime-512x512-quench", dim=2, spin=2, n=(512, 512, 1), d=(0.05, 0.05, 1.0),
+           dt=1e-4, mass=87.0, a=(87.93, 91.28, 99.18), natoms=50000, nu=(20.0, 20.0, 500.0),
+           gamma=(1.2, 1.0, 0.0), switch_im=0, seed=2)
+WORKLOADS = {"3d": D3, "q2d": Q2D}
 
-def workload_config(gamma):
+
+def run_config(w, n=None, d=None):
     from fortress_b200.config import RunConfig
-    w = WORKLOAD
-    c = RunConfig(dim=2, spin=2, n=(512, 512, 1), d=(0.05, 0.05, 1.0), dt=w["dt"], mass=w["mass"],
-                  a=w["a"], natoms=w["natoms"], nu=w["nu"], switch_im=0,
-                  gamma=(gamma[0], gamma[1], 0.0))
-    return c
+    return RunConfig(dim=w["dim"], spin=w["spin"], n=n or w["n"], d=d or w["d"], dt=w["dt"], mass=w["mass"],
+                     a=w["a"], natoms=w["natoms"], nu=w["nu"], switch_im=w["switch_im"], gamma=w["gamma"])
 
 
-def gaussian_guess(cfg):
-    """INITIALIZE default spin-2 guess, cgpe2d.f90:766-771."""
+def initial_state(w, n=None, d=None):
+    """The workload's synthetic start, PHI(NX,NY,NZ,M) complex128.
+    3D: INITIALIZE's default spin-1 guess exp(-(x^2+y^2+z^2)/2)/pi^(3/4) in
+    every component (cgpe3d.f90:783-785) times (1 + 1e-3 u), u ~ U[0,1).
+    q2D: the spin-2 default sqrt(0.2) exp(-(ax x^2 + ay y^2)/2)/sqrt(pi)
+    (cgpe2d.f90:766-771) plus 1e-3 of its peak in complex Gaussian noise."""
     import numpy as np
-    nx, ny = cfg.n[0], cfg.n[1]
-    x = (-1.0 + 2.0 * np.arange(nx) / nx) * nx * cfg.d[0] / 2.0
-    y = (-1.0 + 2.0 * np.arange(ny) / ny) * ny * cfg.d[1] / 2.0
-    ax, ay, _ = cfg.alpha
-    g = np.sqrt(0.2) * np.exp(-(ax * x[:, None] ** 2 + ay * y[None, :] ** 2) / 2.0) / np.sqrt(np.pi)
-    return np.repeat(g[:, :, None], 5, axis=2).astype(np.complex128)
+    n = n or w["n"]
+    d = d or w["d"]
+    ms = 2 * w["spin"] + 1
+    rng = np.random.default_rng(w["seed"])
+    ax = [(-1.0 + 2.0 * np.arange(n[a]) / n[a]) * n[a] * d[a] / 2.0 for a in range(w["dim"])]
+    if w["dim"] == 3:
+        r2 = ax[0][:, None, None] ** 2 + ax[1][None, :, None] ** 2 + ax[2][None, None, :] ** 2
+        g = np.exp(-r2 / 2.0) / np.pi ** 0.75
+        phi = np.empty(tuple(n) + (ms,), np.complex128)
+        for m in range(ms):
+            phi[..., m] = g * (1.0 + 1e-3 * rng.uniform(size=g.shape))
+        return phi
+    nu = w["nu"]
+    al = (1.0, nu[1] / nu[0])
+    g = np.sqrt(0.2) * np.exp(-(al[0] * ax[0][:, None] ** 2 + al[1] * ax[1][None, :] ** 2) / 2.0) / np.sqrt(np.pi)
+    phi = np.repeat(g[:, :, None, None], ms, axis=3).astype(np.complex128)
+    return phi + 1e-3 * np.abs(phi).max() * (rng.standard_normal(phi.shape) + 1j * rng.standard_normal(phi.shape))
 
 
-def add_noise(phi, seed=2):
-    import numpy as np
-    rng = np.random.default_rng(seed)
-    phi = phi + 1e-3 * (rng.standard_normal(phi.shape) + 1j * rng.standard_normal(phi.shape)) * np.abs(phi).max()
-    return phi
+def bench_config(w, precision="fp64", world=1, impl="ours"):
+    """The config object both arms print (the driver compares them)."""
+    return {"workload": w["name"], "grid": list(w["n"][:w["dim"]]), "spin": w["spin"],
+            "components": 2 * w["spin"] + 1, "time": "imaginary" if w["switch_im"] else "real",
+            "dt": w["dt"], "gamma": list(w["gamma"][:w["dim"]]), "precision": precision,
+            "parallelism": f"replicas{world}" if world > 1 else "single",
+            "l2": "state larger than L2 (not flushed)" if w is D3 else "flushed before every timed step (256 MiB write)"}
 
 
-def prepared_state(F, cfg_gs, prep_steps=3000):
-    """Ground-state-like start: imaginary time on the device from the guess."""
-    import numpy as np
-    p = cfg_gs.params()
-    p["imag_time"] = True
-    p["dt"] = 1e-3
-    prop = F.Propagator(**p)
-    prop.set_state(gaussian_guess(cfg_gs))
-    prop.normt()
-    prop.step(prep_steps)
-    phi = add_noise(prop.state().reshape(512, 512, 5))
-    prop.close()
-    # renormalise to the Simpson norm 1 (NORMT of the reference)
-    from fortress_b200.config import simpson_weights
-    w = simpson_weights(512, cfg_gs.d[0])
-    tot = float(np.einsum("i,j,ijm->", w, w, np.abs(phi) ** 2))
-    return phi / np.sqrt(tot)
-
+def data_string(w):
+    if w is D3:
+        return "synthetic: INITIALIZE's 3D spin-1 Gaussian x (1 + 1e-3 U[0,1), PCG64 seed 3), NORMT"
+    return "synthetic: INITIALIZE's q2D spin-2 Gaussian + 1e-3 complex Gaussian noise (PCG64 seed 2), quench"
 
 # ------------------------------------------------------------------ clocks
 def out_dir():
@@ -157,42 +171,80 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
-def known_traffic(workload, precision, kernel):
+def profile_figures(workload, precision, kernel):
+    """Per-launch DRAM traffic and FP64 operation count of a kernel, from the
+    committed ncu summaries (profiles/traffic.json: dram__bytes_read.sum +
+    dram__bytes_write.sum, and the FP64 flops from the dadd/dmul/dfma
+    instruction counts, per launch, scaled to the bench grid where the
+    capture ran on a smaller one).  (None, None) when not captured."""
     path = os.path.join(ROOT, "profiles", "traffic.json")
     try:
         with open(path) as f:
             d = json.load(f)
-        return d.get(f"{workload}/{precision}/{kernel}")
+        e = d.get(f"{workload}/{precision}/{kernel}")
     except Exception:
-        return None
+        return None, None
+    if e is None:
+        return None, None
+    if isinstance(e, dict):
+        return e.get("dram_bytes"), e.get("fp64_flops")
+    return e, None
+
+
+def fp64_peak_tflops():
+    """Measured FP64 FMA throughput of this device (fgpe_fp64_fma_rate)."""
+    from fortress_b200 import _abi
+    t = ctypes.c_double()
+    rc = _abi.load().fgpe_fp64_fma_rate(200000, ctypes.byref(t))
+    return float(t.value) if rc == 0 else None
+
+
 
 
 # --------------------------------------------------------------- CPU legs
-def run_cpu(phi, cfg, steps, warmup, budget_s=None):
+def oracle_for(w, phi):
+    """The oracle on the workload's parameters, holding phi."""
     from oracle import oracle as O
+    cfg = run_config(w)
     t = cfg.tau()
-    orc = O.Oracle(dim=2, spin=2, nx=512, ny=512, dx=cfg.d[0], dy=cfg.d[1], dt=cfg.dt, imag=0, tau=t,
-                   gx=cfg.gamma[0], gy=cfg.gamma[1], ax=cfg.alpha[0], ay=cfg.alpha[1], az=cfg.alpha[2])
+    n, d, g, al = cfg.n, cfg.d, cfg.gamma, cfg.alpha
+    orc = O.Oracle(dim=w["dim"], spin=w["spin"], nx=n[0], ny=n[1], nz=n[2], dx=d[0], dy=d[1], dz=d[2],
+                   dt=cfg.dt, imag=int(cfg.switch_im), tau=t, gx=g[0], gy=g[1], gz=g[2],
+                   ax=al[0], ay=al[1], az=al[2])
     orc.set_state(phi)
+    if cfg.switch_im:
+        orc.normt()
+    return orc, O.num_threads()
+
+
+def run_cpu(w, phi, steps, warmup, budget_s):
+    """Oracle split steps on the host cores: warm-up steps, then up to
+    `steps` timed steps, stopping after budget_s seconds (at least one)."""
+    orc, thr = oracle_for(w, phi)
     for _ in range(warmup):
         orc.step(1)
+    npts = int(w["n"][0] * w["n"][1] * w["n"][2])
     done, t0 = 0, time.perf_counter()
     while done < steps:
         orc.step(1)
         done += 1
-        if budget_s is not None and time.perf_counter() - t0 > budget_s and done >= 2:
+        if time.perf_counter() - t0 > budget_s:
             break
     el = time.perf_counter() - t0
-    return 512 * 512 * done / el, done, el, O.num_threads()
+    del orc
+    return npts * done / el, done, el, thr
 
 
 def capture(args):
     """The step kernels alone, for ncu launch lists and per-kernel captures
-    (-k regex:k_row_fast / k_col_fast): warmup + steps split steps of the
-    512^2 spin-2 real-time case from the noisy Gaussian guess, or with
-    --workload 3d of the 3D spin-1 case on a 128^3 grid (the same kernel
-    families, wide column tiles included, at an eighth of the 256^3 state:
-    a small case for ncu)."""
+    (-k regex:k_row_fast / k_col_fast / k_obs ...): warmup + steps split
+    steps of the workload on its initial state, no timing and no other work.
+    --workload 3d runs the 3D spin-1 case on --grid^3 points (default 192:
+    the same kernel families as 256^3, wide column tiles included, with a
+    340 MB state that still exceeds L2, for DRAM figures that scale to the
+    bench grid); --workload q2d the 512^2 spin-2 real-time case; --workload
+    fno learned-guess training steps; --workload golden1d the reference's
+    published 1D run."""
     import numpy as np
     import fortress_b200 as F
     if args.workload == "fno":
@@ -223,29 +275,25 @@ def capture(args):
         assert np.isfinite(en)
         print(json.dumps({"capture": "golden-1d-spin2-2048", "steps": args.warmup + args.steps, "en": en}))
         return
-    if args.workload == "3d":
-        from fortress_b200.config import RunConfig
-        w = D3
-        cfg = RunConfig(dim=3, spin=1, n=(128, 128, 128), d=(0.2, 0.2, 0.2), dt=w["dt"], mass=w["mass"],
-                        a=w["a"], natoms=w["natoms"], nu=w["nu"], switch_im=1, gamma=w["gamma"])
-        p = cfg.params(args.precision)
-        prop = F.Propagator(**p)
-        prop.set_state(gaussian_nd(p))
-        prop.normt()
-        prop.step(args.warmup + args.steps, snapshot=False)
-        n = prop.normc()
-        assert np.all(np.isfinite(n))
-        print(json.dumps({"capture": "3d-spin1-SO-imag-128^3", "precision": args.precision,
-                          "steps": args.warmup + args.steps, "norm": float(n.sum())}))
-        return
-    cfg = workload_config(WORKLOAD["gamma"])
+    w = WORKLOADS[args.workload]
+    if w is D3:
+        g = args.grid or 192
+        n, d = (g, g, g), (25.6 / g,) * 3
+    else:
+        n, d = w["n"], w["d"]
+    cfg = run_config(w, n, d)
     prop = F.Propagator(**cfg.params(args.precision))
-    prop.set_state(add_noise(gaussian_guess(cfg)))
+    prop.set_state(initial_state(w, n, d))
+    if cfg.switch_im:
+        prop.normt()
     prop.step(args.warmup + args.steps, snapshot=False)
-    n = prop.normc()
-    assert np.all(np.isfinite(n))
-    print(json.dumps({"capture": WORKLOAD["name"], "precision": args.precision,
-                      "steps": args.warmup + args.steps, "norm": float(n.sum())}))
+    if args.observables:
+        en = prop.observables()[0]
+        assert np.isfinite(en)
+    nrm = prop.normc()
+    assert np.all(np.isfinite(nrm))
+    print(json.dumps({"capture": w["name"], "grid": list(n[:w["dim"]]), "precision": args.precision,
+                      "steps": args.warmup + args.steps, "norm": float(nrm.sum())}))
 
 
 def kernel_pass(prop, flush, steps):
@@ -256,7 +304,8 @@ def kernel_pass(prop, flush, steps):
     prop.profile(True)
     prop.profile_read(reset=True)
     for _ in range(steps):
-        flush.zero_()
+        if flush is not None:
+            flush.zero_()
         prop.step(1, snapshot=False)
     torch.cuda.synchronize()
     kms, kn = prop.profile_read(reset=True)
@@ -264,41 +313,117 @@ def kernel_pass(prop, flush, steps):
     return kms, kn
 
 
+KCLASS = ["row_x", "col_y", "col_z", "oned"]
+
+
+def device_rate(F, w, phi, precision, steps, warmup, stream, flush, world, dist):
+    """value of one precision: K split steps on the device between CUDA
+    events on the launching stream (max over ranks), plus the per-kernel
+    pass.  Returns a dict and the propagator."""
+    import numpy as np
+    import torch
+    cfg = run_config(w)
+    prop = F.Propagator(**cfg.params(precision))
+    prop.set_stream(stream.cuda_stream)
+    prop.set_state(phi)
+    if cfg.switch_im:
+        prop.normt()
+    npts = int(np.prod(w["n"]))
+    for _ in range(warmup):
+        if flush is not None:
+            flush.zero_()
+        prop.step(1, snapshot=False)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = prop.kernel_launches()
+    if flush is None:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            prop.step(1, snapshot=False)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        total_ms = e0.elapsed_time(e1)
+    else:
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for k in range(steps):
+            flush.zero_()
+            evs[k][0].record(stream)
+            prop.step(1, snapshot=False)
+            evs[k][1].record(stream)
+        torch.cuda.synchronize()
+        total_ms = sum(a.elapsed_time(b) for a, b in evs)
+    launches = prop.kernel_launches() - l0
+    if dist:
+        dist.barrier()
+        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    kms, kn = kernel_pass(prop, flush, steps)
+    return {"value": world * npts * steps / (total_ms / 1e3), "ms_per_step": total_ms / steps,
+            "launches": int(launches), "kms": kms, "kn": kn}, prop
+
+
+def roofline(w, precision, kms, kn, peak, peak_kind, fp64_peak):
+    """HBM roofline of the dominant kernel class (algorithmic bytes per
+    launch = the spinor read and written once, 2*M*N*s) and its FP64
+    compute fraction against the measured FP64 FMA peak."""
+    import numpy as np
+    npts = int(np.prod(w["n"]))
+    ms_comp = 2 * w["spin"] + 1
+    cs = 16 if precision == "fp64" else 8
+    dom = int(np.argmax(kms))
+    per_launch_ms = kms[dom] / max(kn[dom], 1)
+    alg = 2 * ms_comp * npts * cs
+    achieved = alg / (per_launch_ms / 1e3) / 1e9
+    traffic, fp64_flops = profile_figures(w["name"], precision, KCLASS[dom])
+    r = {"bound": "hbm", "kernel": KCLASS[dom], "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
+         "unit": "GB/s", "frac": achieved / peak, "traffic": traffic, "alg_bytes_per_launch": alg,
+         "ms_per_launch": per_launch_ms}
+    if fp64_flops and fp64_peak:
+        tf = fp64_flops / (per_launch_ms / 1e3) / 1e12
+        r["fp64"] = {"achieved": tf, "peak": fp64_peak, "unit": "TFLOP/s", "frac": tf / fp64_peak,
+                     "flops_per_launch": fp64_flops, "peak_kind": "measured (fgpe_fp64_fma_rate, this run)"}
+    kernels = {KCLASS[i]: {"launches": int(kn[i]), "ms_per_launch": float(kms[i] / kn[i]),
+                           "share": float(kms[i] / kms.sum())} for i in range(4) if kn[i]}
+    return r, kernels
+
+
+def e2e_rate(prop, w, phi_host, out_host, norms_host, steps, world, dist):
+    """The public API with host buffers on a host wall clock: upload, K
+    steps (each writes its NORMC into the pinned ring), download, sync."""
+    import numpy as np
+    import torch
+    ms_comp = 2 * w["spin"] + 1
+    npts = int(np.prod(w["n"]))
+    prop.norms_sink(norms_host.data_ptr(), steps)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    prop.set_state_host_ptr(phi_host.data_ptr())
+    if w["switch_im"]:
+        prop.normt()
+    prop.step(steps, snapshot=True)
+    prop.get_state_host_ptr(out_host.data_ptr())     # synchronises the stream
+    el = time.perf_counter() - t0
+    prop.norms_sink(0, 0)
+    norms = norms_host.numpy().reshape(steps, ms_comp)
+    assert np.all(np.isfinite(norms)) and np.all(np.isfinite(out_host.numpy()[:1024]))
+    if dist:
+        t = torch.tensor([el], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        el = float(t.item())
+    state_bytes = npts * ms_comp * 16
+    return {"value": world * npts * steps / el, "unit": METRIC, "wall_s": el,
+            "h2d_bytes_per_step": state_bytes / steps, "d2h_bytes_per_step": 8 * ms_comp + state_bytes / steps,
+            "timing": "host wall clock around upload, steps, per-step NORMC ring and download"}
+
+
 # -------------------------------------------------------------------- main
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
-    ap.add_argument("--warmup", type=int, default=10)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
-    ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--prep-steps", type=int, default=3000,
-                    help="imaginary-time relaxation steps that build the initial state (untimed)")
-    ap.add_argument("--workload", default="q2d", choices=["q2d", "3d", "sweep", "golden1d", "fno"],
-                    help="q2d: 512^2 spin-2 real time (headline); 3d: 256^3 spin-1 imaginary time; "
-                         "sweep: 512 ragged q2D spin-1 instances in one batched graph launch; "
-                         "golden1d: the reference's published run (1D spin-2, 2048 points, to convergence); "
-                         "fno: with --capture only, learned-guess training steps")
-    ap.add_argument("--capture", action="store_true",
-                    help="run only the workload's step kernels (warmup + steps launches of each, on the "
-                         "unrelaxed guess, no timing, no other work) for profiler captures")
-    args = ap.parse_args()
-    args.warmup = max(args.warmup, 3)
-    if args.capture:
-        return capture(args)
-    if args.workload == "fno" and not args.capture:
-        ap.error("--workload fno is a profiling case: use it with --capture")
-    if args.workload != "q2d" and args.impl == "ours":
-        return other_workload(args)
-
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
-
-    if args.impl == "reference":
-        return reference_arm(args, rank, world)
-
+def ours(args, w, rank, world, local_rank):
     import numpy as np
     import torch
     torch.cuda.set_device(local_rank)
@@ -310,134 +435,50 @@ def main():
                                 device_id=torch.device("cuda", local_rank))
     import fortress_b200 as F
 
-    cfg_gs = workload_config(WORKLOAD["gamma_gs"])
-    cfg = workload_config(WORKLOAD["gamma"])
-    phi0 = prepared_state(F, cfg_gs, args.prep_steps)
-
-    prop = F.Propagator(**cfg.params(args.precision))
+    phi = initial_state(w)
+    npts = int(np.prod(w["n"]))
+    ms_comp = 2 * w["spin"] + 1
     # a real (non-default) stream shared by torch's events and the library
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
-    prop.set_stream(stream.cuda_stream)
-    prop.set_state(phi0)
-    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
-    npts = 512 * 512
-    ms_comp, cs = 5, (16 if args.precision == "fp64" else 8)
+    flush = None if w is D3 else torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    peak, peak_kind = measured_peaks()
+    fp64_peak = fp64_peak_tflops()
 
-    for _ in range(args.warmup):
-        flush.zero_()
-        prop.step(1, snapshot=False)
-    torch.cuda.synchronize()
-
-    # ---------------------------------------------------------- value
-    # (per-kernel events cost about 10 us of device time per step, so the
-    # value is timed without them; kernel_pass() below times the kernels)
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     clocks = ClockSampler(local_rank)
     clocks.start()
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    l0 = prop.kernel_launches()
-    for k in range(args.steps):
-        flush.zero_()
-        evs[k][0].record(stream)
-        prop.step(1, snapshot=False)
-        evs[k][1].record(stream)
-    torch.cuda.synchronize()
-    launches = prop.kernel_launches() - l0
-    if dist:
-        dist.barrier()
+    main, prop = device_rate(F, w, phi, args.precision, args.steps, args.warmup, stream, flush, world, dist)
     clk = clocks.stop()
-    total_ms = sum(a.elapsed_time(b) for a, b in evs)
-    kms, kn = kernel_pass(prop, flush, args.steps)
-    t_max = total_ms
-    if dist:
-        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max = float(t.item())
-    value = world * npts * args.steps / (t_max / 1e3)
+    rl, kernels = roofline(w, args.precision, main["kms"], main["kn"], peak, peak_kind, fp64_peak)
 
-    # --------------------------------------------------- e2e (host buffers)
+    # e2e through the C ABI with host buffers (FP64 state in PHI layout)
     phi_host = torch.empty(npts * ms_comp * 2, dtype=torch.float64, pin_memory=True)
-    phi_host.numpy()[:] = np.ascontiguousarray(phi0.reshape(-1, order="F")).view(np.float64)
+    phi_host.numpy()[:] = np.ascontiguousarray(phi.reshape(-1, order="F")).view(np.float64)
     out_host = torch.empty_like(phi_host).pin_memory()
     norms_host = torch.empty(args.steps * ms_comp, dtype=torch.float64, pin_memory=True)
-    # every step writes its NORMC straight into this pinned ring (the step's
-    # device-to-host result read), without a call or a kernel of its own
-    prop.norms_sink(norms_host.data_ptr(), args.steps)
-    e2e_ms = 0.0
-    torch.cuda.synchronize()
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * args.steps + 4)]
-    flush.zero_()
-    ev[0].record(stream)
-    prop.set_state_host_ptr(phi_host.data_ptr())
-    ev[1].record(stream)
-    for k in range(args.steps):
-        if k:
-            flush.zero_()
-        ev[2 + 2 * k].record(stream)
-        prop.step(1, snapshot=(k == args.steps - 1))
-        ev[3 + 2 * k].record(stream)
-    flush.zero_()
-    ev[2 * args.steps + 2].record(stream)
-    prop.get_state_host_ptr(out_host.data_ptr())
-    ev[2 * args.steps + 3].record(stream)
-    torch.cuda.synchronize()
-    prop.norms_sink(0, 0)
-    e2e_ms = ev[0].elapsed_time(ev[1]) + ev[2 * args.steps + 2].elapsed_time(ev[2 * args.steps + 3])
-    e2e_ms += sum(ev[2 + 2 * k].elapsed_time(ev[3 + 2 * k]) for k in range(args.steps))
-    norms = norms_host.numpy().reshape(args.steps, ms_comp)
-    # Real time conserves the discrete l2 norm; NORMC integrates with Simpson
-    # weights, which the evolution does not conserve exactly once the state
-    # carries grid-scale structure (the seeded noise), so the drift of that
-    # norm is reported and only bounded loosely here.
-    norm_drift = float(abs(norms[-1].sum() - norms[0].sum()) / norms[0].sum())
-    assert np.all(np.isfinite(norms)) and norm_drift < 1e-2, norm_drift
-    if dist:
-        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = world * npts * args.steps / (e2e_ms / 1e3)
-    state_bytes = npts * ms_comp * 16
-
-    # ------------------------------------------------------------ roofline
-    classes = ["row_x", "col_y", "col_z", "oned"]
-    dom = int(np.argmax(kms))
-    per_launch_ms = kms[dom] / max(kn[dom], 1)
-    alg_bytes = 2 * ms_comp * npts * cs               # read + write of the spinor
-    peak, peak_kind = measured_peaks()
-    achieved = alg_bytes / (per_launch_ms / 1e3) / 1e9
-    kernels = {classes[i]: {"launches": int(kn[i]), "ms_per_launch": float(kms[i] / kn[i]),
-                            "share": float(kms[i] / kms.sum())} for i in range(4) if kn[i]}
+    e2e = e2e_rate(prop, w, phi_host, out_host, norms_host, args.steps, world, dist)
+    prop.close()
 
     result = {
-        "metric": METRIC, "value": value, "unit": "grid-pt*steps/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps,
+        "metric": METRIC, "value": main["value"], "unit": METRIC, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": main["ms_per_step"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "c128" if args.precision == "fp64" else "c64",
-        "data": "synthetic (relaxed Gaussian guess + seeded noise)",
-        "config": {"workload": WORKLOAD["name"], "grid": [512, 512], "spin": 2, "components": 5,
-                   "time": "real", "dt": WORKLOAD["dt"], "precision": args.precision,
-                   "parallelism": f"replicas{world}" if world > 1 else "single",
-                   "l2": "flushed before every timed step (256 MiB write)",
-                   "kernel_times": "second timed pass of the same steps with per-kernel CUDA events"},
-        "e2e": {"value": e2e_value, "unit": "grid-pt*steps/s",
-                "h2d_bytes_per_step": state_bytes / args.steps,
-                "d2h_bytes_per_step": 8 * ms_comp + state_bytes / args.steps,
-                "simpson_norm_drift": norm_drift},
-        "gpu_launches": int(launches),
-        "roofline": {"bound": "hbm", "kernel": classes[dom], "achieved": achieved, "peak": peak,
-                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": known_traffic(WORKLOAD["name"], args.precision, classes[dom]),
-                     "alg_bytes_per_launch": alg_bytes},
-        "kernels": kernels,
-        "clocks": clk,
+        "dtype": "c128" if args.precision == "fp64" else "c64", "data": data_string(w),
+        "config": bench_config(w, args.precision, world),
+        "e2e": e2e, "gpu_launches": main["launches"], "roofline": rl, "kernels": kernels, "clocks": clk,
     }
+    if args.precision == "fp64" and not args.no_fp32:
+        f32, p32 = device_rate(F, w, phi, "fp32", args.steps, args.warmup, stream, flush, world, dist)
+        p32.close()
+        rl32, k32 = roofline(w, "fp32", f32["kms"], f32["kn"], peak, peak_kind, fp64_peak)
+        result["fp32"] = {"value": f32["value"], "ms_per_step": f32["ms_per_step"], "dtype": "c64",
+                          "what": "FP32 bulk: complex64 FFTs and exponentials, FP64 reductions and NORMT",
+                          "gpu_launches": f32["launches"], "roofline": rl32, "kernels": k32}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        rate, done, el, thr = run_cpu(phi0, cfg, steps=30, warmup=1, budget_s=12.0)
-        result["cpu_baseline"] = {"value": rate, "unit": "grid-pt*steps/s", "cores": thr, "kind": "port",
-                                  "sample": f"{done} steps of the same 512^2 workload ({el:.1f} s, oracle/ FP64 OpenMP)"}
+        rate, done, el, thr = run_cpu(w, phi, steps=30, warmup=0, budget_s=20.0)
+        result["cpu_baseline"] = {"value": rate, "unit": METRIC, "cores": thr, "kind": "port",
+                                  "sample": f"{done} split steps of the same workload from the same state "
+                                            f"({el:.1f} s, oracle/ FP64 OpenMP on {thr} threads)"}
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -445,11 +486,28 @@ def main():
         print(json.dumps(result))
 
 
+def reference_arm(args, w, rank, world):
+    """The reference's algorithm on the host cores (the oracle port: the
+    Fortran reference cannot be built here), same workload, state and
+    config; each timed step is one whole split step of the full grid."""
+    if rank != 0:
+        return 0
+    phi = initial_state(w)
+    warm = min(args.warmup, 1)
+    rate, done, el, thr = run_cpu(w, phi, steps=args.steps, warmup=warm, budget_s=90.0)
+    res = {"metric": METRIC, "value": rate, "unit": METRIC, "n_gpus": world, "steps": done,
+           "warmup": args.warmup, "ms_per_step": 1e3 * el / done, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "c128" if args.precision == "fp64" else "c64",
+           "impl": "reference", "data": data_string(w), "config": bench_config(w, args.precision, world),
+           "cpu_baseline": {"value": rate, "unit": METRIC, "cores": thr, "kind": "port",
+                            "sample": f"{done} timed split steps after {warm} warm-up step(s), "
+                                      f"at most 90 s (oracle/ FP64 OpenMP on {thr} threads)"},
+           "e2e": {"value": rate, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(res))
+    return 0
+
+
 # ------------------------------------------------------- other workloads
-D3 = dict(name="3d-spin1-SO-imag-256^3", n=(256, 256, 256), d=(0.1, 0.1, 0.1), dt=1e-3, mass=87.0,
-          a=(101.8, 100.4, 0.0), natoms=100000, nu=(50.0, 50.0, 50.0), gamma=(0.5, 0.5, 0.5))
-
-
 def sweep_instances(count=512, seed=4, precision="fp32"):
     """Seeded parameter box of the phase-diagram sweep: sizes from
     {128,192,256,384,512}^2, GAMMAX/GAMMAY in [0,2], c0 in [100,2000],
@@ -483,6 +541,7 @@ def gaussian_nd(p):
     g = np.exp(-r2 / 2.0)
     ms = 2 * p["spin"] + 1
     return np.repeat(g[..., None], ms, axis=-1).astype(np.complex128)
+
 
 
 # Wall time of the reference's own published run (its OUTPUT/ folder): 1D
@@ -529,67 +588,15 @@ def golden1d(args):
                       "clocks": clk}))
 
 
-def other_workload(args):
+
+def sweep(args):
+    """512 ragged q2D spin-1 instances (seed 4) advanced by the batched
+    launcher after its autotuner has picked the launch shape."""
     import numpy as np
-    import torch
-    import fortress_b200 as F
-    if args.workload == "golden1d":
-        return golden1d(args)
-    from fortress_b200.config import RunConfig
-    peak, peak_kind = measured_peaks()
-    clocks = ClockSampler(0)
-    if args.workload == "3d":
-        w = D3
-        cfg = RunConfig(dim=3, spin=1, n=w["n"], d=w["d"], dt=w["dt"], mass=w["mass"], a=w["a"],
-                        natoms=w["natoms"], nu=w["nu"], switch_im=1, gamma=w["gamma"])
-        prop = F.Propagator(**cfg.params(args.precision))
-        s = torch.cuda.Stream(); torch.cuda.set_stream(s); prop.set_stream(s.cuda_stream)
-        p = cfg.params(args.precision)
-        phi = gaussian_nd(p)
-        rng = np.random.default_rng(3)
-        phi *= 1.0 + 1e-3 * rng.uniform(size=phi.shape)
-        prop.set_state(phi)
-        prop.normt()
-        npts = int(np.prod(w["n"]))
-        flush = torch.empty(256 * 2 ** 20, dtype=torch.uint8, device="cuda")
-        for _ in range(args.warmup):
-            flush.zero_(); prop.step(1, snapshot=False)
-        torch.cuda.synchronize()
-        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-        l0 = prop.kernel_launches()
-        clocks.start()
-        for k in range(args.steps):
-            flush.zero_()
-            evs[k][0].record(s); prop.step(1, snapshot=False); evs[k][1].record(s)
-        torch.cuda.synchronize()
-        clk = clocks.stop()
-        total_ms = sum(a.elapsed_time(b) for a, b in evs)
-        launches = prop.kernel_launches() - l0
-        kms, kn = kernel_pass(prop, flush, args.steps)
-        cs = 16 if args.precision == "fp64" else 8
-        alg = 2 * 3 * npts * cs
-        classes = ["row_x", "col_y", "col_z", "oned"]
-        dom = int(np.argmax(kms))
-        achieved = alg / (kms[dom] / kn[dom] / 1e3) / 1e9
-        res = {"metric": METRIC, "value": npts * args.steps / (total_ms / 1e3), "unit": "grid-pt*steps/s",
-               "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
-               "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-               "dtype": "c128" if args.precision == "fp64" else "c64", "data": "synthetic (seeded Gaussian guess)",
-               "config": {"workload": w["name"], "precision": args.precision, "time": "imaginary",
-                          "l2": "flushed before every timed step (state also larger than L2)",
-                          "kernel_times": "second timed pass of the same steps with per-kernel CUDA events"},
-               "gpu_launches": int(launches),
-               "roofline": {"bound": "hbm", "kernel": classes[dom], "achieved": achieved, "peak": peak,
-                            "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
-                            "alg_bytes_per_launch": alg},
-               "kernels": {classes[i]: {"launches": int(kn[i]), "ms_per_launch": float(kms[i] / kn[i]),
-                                        "share": float(kms[i] / kms.sum())} for i in range(4) if kn[i]},
-               "clocks": clk}
-        print(json.dumps(res))
-        return 0
-    # sweep
     from fortress_b200.batch import Batch
-    insts = sweep_instances(precision=args.precision)
+    peak, _ = measured_peaks()
+    clocks = ClockSampler(0)
+    insts = sweep_instances(precision=args.precision if args.precision_set else "fp32")
     b = Batch(insts)
     for i, p in enumerate(insts):
         b[i].set_state(gaussian_nd(p))
@@ -600,42 +607,70 @@ def other_workload(args):
     clocks.start()
     steps = args.steps + (1 if args.steps % tune[1] == 1 else 0)   # whole graph launches only
     el = b.step_timed(steps) / 1e3                                # CUDA events on the launch stream
-    args.steps = steps
     clk = clocks.stop()
-    cs = 16 if args.precision == "fp64" else 8
-    res = {"metric": METRIC, "value": npts * args.steps / el, "unit": "grid-pt*steps/s", "n_gpus": 1,
-           "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+    prec = insts[0]["precision"]
+    cs = 16 if prec == "fp64" else 8
+    alg = 2 * 2 * 3 * npts * cs
+    res = {"metric": METRIC, "value": npts * steps / el, "unit": METRIC, "n_gpus": 1,
+           "steps": steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / steps,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-           "dtype": "c128" if args.precision == "fp64" else "c64", "data": "synthetic (seeded parameter box, seed 4)",
+           "dtype": "c128" if prec == "fp64" else "c64", "data": "synthetic (seeded parameter box, seed 4)",
            "config": {"workload": "sweep-512-ragged-q2d-spin1-imag", "instances": len(insts),
-                      "sizes": sorted(set(p["n"][0] for p in insts)), "precision": args.precision,
+                      "sizes": sorted(set(p["n"][0] for p in insts)), "precision": prec,
                       "autotuned": {"width": tune[0], "steps_per_graph": tune[1]},
-                      "hbm_bytes_per_step_alg": 2 * 2 * 3 * npts * cs,
                       "l2": "batch state larger than L2"},
-           "achieved_gbs_alg": 2 * 2 * 3 * npts * cs / (el / args.steps) / 1e9, "peak": peak,
+           "roofline": {"bound": "hbm", "kernel": "whole batch step", "achieved": alg / (el / steps) / 1e9,
+                        "peak": peak, "unit": "GB/s", "frac": alg / (el / steps) / 1e9 / peak,
+                        "alg_bytes_per_step": alg},
            "clocks": clk}
     print(json.dumps(res))
     return 0
 
 
-def reference_arm(args, rank, world):
-    if rank != 0:
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default=None, choices=["fp64", "fp32"],
+                    help="arithmetic of the headline value (default fp64; the fp32 figure is added beside it)")
+    ap.add_argument("--no-fp32", action="store_true", help="skip the FP32-bulk figure")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="3d", choices=["3d", "q2d", "sweep", "golden1d", "fno"],
+                    help="3d: 256^3 spin-1 imaginary time (headline); q2d: 512^2 spin-2 real-time quench; "
+                         "sweep: 512 ragged q2D spin-1 instances in one batched graph launch; "
+                         "golden1d: the reference's published run (1D spin-2, 2048 points, to convergence); "
+                         "fno: with --capture only, learned-guess training steps")
+    ap.add_argument("--capture", action="store_true",
+                    help="run only the workload's step kernels (warmup + steps launches of each, no timing, "
+                         "no other work) for profiler captures")
+    ap.add_argument("--grid", type=int, default=0, help="with --capture --workload 3d: points per axis (192)")
+    ap.add_argument("--observables", action="store_true", help="with --capture: also run ENERGY/RAD (k_obs)")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    args.precision_set = args.precision is not None
+    args.precision = args.precision or "fp64"
+    if args.capture:
+        return capture(args)
+    if args.workload == "fno":
+        ap.error("--workload fno is a profiling case: use it with --capture")
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.workload in WORKLOADS:
+        w = WORKLOADS[args.workload]
+        if args.impl == "reference":
+            return reference_arm(args, w, rank, world)
+        return ours(args, w, rank, world, local_rank)
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps({"impl": "reference", "unavailable": f"--impl reference covers the 3d and q2d "
+                                                                  f"workloads, not {args.workload}"}))
         return 0
-    import numpy as np  # noqa: F401
-    cfg = workload_config(WORKLOAD["gamma"])
-    phi = add_noise(gaussian_guess(cfg))
-    rate, done, el, thr = run_cpu(phi, cfg, steps=args.steps, warmup=args.warmup, budget_s=90.0)
-    res = {"metric": METRIC, "value": rate, "unit": "grid-pt*steps/s", "n_gpus": world, "steps": done,
-           "warmup": args.warmup, "ms_per_step": 1e3 * el / done, "higher_is_better": True,
-           "scaling": "weak", "vs_baseline": None, "dtype": "c128", "impl": "reference",
-           "data": "synthetic (Gaussian guess + seeded noise)",
-           "config": {"workload": WORKLOAD["name"], "grid": [512, 512], "spin": 2, "time": "real",
-                      "precision": "fp64", "parallelism": "cpu"},
-           "cpu_baseline": {"value": rate, "unit": "grid-pt*steps/s", "cores": thr, "kind": "port",
-                            "sample": f"{done} timed steps after {args.warmup} warm-up steps"},
-           "e2e": {"value": rate, "unit": "grid-pt*steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(res))
-    return 0
+    if args.workload == "golden1d":
+        return golden1d(args)
+    return sweep(args)
 
 
 if __name__ == "__main__":

@@ -39,6 +39,7 @@ EXPORTS = (
     "fgpe_batch_last_error", "fgpe_batch_config", "fgpe_batch_step", "fgpe_batch_observables",
     "fgpe_batch_autotune", "fgpe_batch_tuning", "fgpe_set_kernels", "fgpe_normc_noalloc",
     "fgpe_checkpoint_save", "fgpe_checkpoint_load", "fgpe_batch_step_timed", "fgpe_norms_sink",
+    "fgpe_fp64_fma_rate",
 )
 
 
@@ -110,6 +111,7 @@ def load():
                                 vp, vp, vp], ip),
         "fgpe_checkpoint_save": ([vp, ctypes.c_char_p, ctypes.c_longlong, dp], ip),
         "fgpe_checkpoint_load": ([vp, ctypes.c_char_p, ctypes.POINTER(ctypes.c_longlong), dp], ip),
+        "fgpe_fp64_fma_rate": ([ip, dp], ip),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

@@ -77,6 +77,7 @@ struct fgpe_s {
     long long launches = 0;
     std::string msg;
     // kernel timing (fgpe_profile_enable)
+    int device = 0;              // ordinal of the device the handle was created on
     bool prof = false;
     std::vector<cudaEvent_t> ev_pool;
     std::vector<std::pair<int, int>> ev_rec;   // (class, pool index of start)
@@ -349,6 +350,7 @@ void launch_col(fgpe_t* h, int axis, int flags) {
     a.tx = h->col[axis].tile;
     a.flags = flags;
     a.n_other = h->p.dim == 2 ? 1 : (axis == 1 ? h->p.nz : h->p.ny);
+    a.axis = axis;
     ProfScope ps(h, axis);
     if (h->fast_col[axis]) {
 #define RUNC(NN) run_fast_col<T, MS, NN>(h, axis, a)
@@ -580,6 +582,7 @@ int fgpe_create(const fgpe_params* pin, fgpe_t** out) {
 
     h = new fgpe_s();
     h->p = p;
+    cudaGetDevice(&h->device);
     h->ms = 2 * p.spin + 1;
     h->npts = (long long)p.nx * p.ny * p.nz;
     h->fp32 = p.precision == FGPE_FP32;
@@ -1046,9 +1049,11 @@ int fgpe_step_ex(fgpe_t* h, int nsteps, int flags) {
         if (h->p.dim == 2) {
             DISPATCH(h, launch_col, h, 1, COL_SCALE | COL_FWD | COL_KOP | COL_INV);
         } else {
+            // KE in the z pass; SO coupling (a function of kx, ky only)
+            // after the inverse z transform, in the inverse y pass
             DISPATCH(h, launch_col, h, 1, COL_SCALE | COL_FWD);
-            DISPATCH(h, launch_col, h, 2, COL_FWD | COL_KOP | COL_INV);
-            DISPATCH(h, launch_col, h, 1, COL_INV);
+            DISPATCH(h, launch_col, h, 2, COL_FWD | COL_KE | COL_INV);
+            DISPATCH(h, launch_col, h, 1, COL_SOC | COL_INV);
         }
         DISPATCH(h, launch_row, h, ROW_FULL, sn);
     };
@@ -1249,11 +1254,9 @@ int fgpe_norms_async(fgpe_t* h, double* dst) {
     // (pageable memory, another device) a copy.
     cudaPointerAttributes at = {};
     double* ddst = nullptr;
-    int cur = 0;
-    CK(cudaGetDevice(&cur));
     if (cudaPointerGetAttributes(&at, dst) == cudaSuccess &&
         ((at.type == cudaMemoryTypeHost && at.devicePointer) ||
-         (at.type == cudaMemoryTypeDevice && at.device == cur)))
+         (at.type == cudaMemoryTypeDevice && at.device == h->device)))
         ddst = (double*)at.devicePointer;
     else
         cudaGetLastError();
@@ -1283,11 +1286,9 @@ int fgpe_norms_sink(fgpe_t* h, double* dst, int count) {
     if (dst) {
         if (count < 1) return fail(h, FGPE_E_ARG, "sink needs at least one record");
         cudaPointerAttributes at = {};
-        int cur = 0;
-        CK(cudaGetDevice(&cur));
         if (cudaPointerGetAttributes(&at, dst) == cudaSuccess &&
             ((at.type == cudaMemoryTypeHost && at.devicePointer) ||
-             (at.type == cudaMemoryTypeDevice && at.device == cur)))
+             (at.type == cudaMemoryTypeDevice && at.device == h->device)))
             ddst = (double*)at.devicePointer;
         cudaGetLastError();
         if (!ddst) return fail(h, FGPE_E_ARG, "sink must be pinned host memory or memory of the handle's device");
@@ -1606,23 +1607,54 @@ int fgpe_batch_autotune(fgpe_batch_t* b, int trial_steps, const char* cache_path
             fclose(f);
         }
     }
-    // save states (spectral buffer or real-space copy, plus the info vector)
+    // save states (spectral buffer or real-space copy, plus the info vector);
+    // every path out of the search below restores them and frees the copies
     std::vector<void*> save(n, nullptr), save_info(n, nullptr);
     std::vector<char> flags(3 * n);
+    int saved = 0;
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    auto finish = [&](int rc) -> int {
+        for (int i = 0; i < saved; ++i) {
+            fgpe_t* h = b->inst[i];
+            const size_t bytes = (size_t)h->npts * h->ms * h->cs;
+            cudaError_t e = cudaStreamSynchronize(h->st);
+            if (e == cudaSuccess) e = cudaMemcpy(h->S, save[i], bytes, cudaMemcpyDeviceToDevice);
+            if (e == cudaSuccess) e = cudaMemcpy(h->psi, (char*)save[i] + bytes, bytes, cudaMemcpyDeviceToDevice);
+            if (e == cudaSuccess) e = cudaMemcpy(h->info, save_info[i], 2 * INFO_LEN * sizeof(double), cudaMemcpyDeviceToDevice);
+            if (e == cudaSuccess) {
+                h->S_valid = flags[3 * i]; h->psi_valid = flags[3 * i + 1]; h->prev_valid = flags[3 * i + 2];
+            } else if (rc == FGPE_OK) {
+                rc = bfail(b, FGPE_E_CUDA, std::string("autotune: restoring instance states: ") + cudaGetErrorString(e));
+            }
+        }
+        for (int i = 0; i < n; ++i) {
+            if (save[i]) cudaFree(save[i]);
+            if (save_info[i]) cudaFree(save_info[i]);
+        }
+        if (t0) cudaEventDestroy(t0);
+        if (t1) cudaEventDestroy(t1);
+        return rc;
+    };
+#define ACK(call)                                                                                   \
+    do {                                                                                            \
+        cudaError_t e_ = (call);                                                                    \
+        if (e_ != cudaSuccess)                                                                      \
+            return finish(bfail(b, FGPE_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_))); \
+    } while (0)
     for (int i = 0; i < n; ++i) {
         fgpe_t* h = b->inst[i];
-        BCK(cudaStreamSynchronize(h->st));
+        ACK(cudaStreamSynchronize(h->st));
         const size_t bytes = (size_t)h->npts * h->ms * h->cs;
-        BCK(cudaMalloc(&save[i], 2 * bytes));
-        BCK(cudaMalloc(&save_info[i], 2 * INFO_LEN * sizeof(double)));
-        BCK(cudaMemcpy(save[i], h->S, bytes, cudaMemcpyDeviceToDevice));
-        BCK(cudaMemcpy((char*)save[i] + bytes, h->psi, bytes, cudaMemcpyDeviceToDevice));
-        BCK(cudaMemcpy(save_info[i], h->info, 2 * INFO_LEN * sizeof(double), cudaMemcpyDeviceToDevice));
+        ACK(cudaMalloc(&save[i], 2 * bytes));
+        ACK(cudaMalloc(&save_info[i], 2 * INFO_LEN * sizeof(double)));
+        ACK(cudaMemcpy(save[i], h->S, bytes, cudaMemcpyDeviceToDevice));
+        ACK(cudaMemcpy((char*)save[i] + bytes, h->psi, bytes, cudaMemcpyDeviceToDevice));
+        ACK(cudaMemcpy(save_info[i], h->info, 2 * INFO_LEN * sizeof(double), cudaMemcpyDeviceToDevice));
         flags[3 * i] = h->S_valid; flags[3 * i + 1] = h->psi_valid; flags[3 * i + 2] = h->prev_valid;
+        saved = i + 1;
     }
-    cudaEvent_t t0, t1;
-    BCK(cudaEventCreate(&t0));
-    BCK(cudaEventCreate(&t1));
+    ACK(cudaEventCreate(&t0));
+    ACK(cudaEventCreate(&t1));
     auto timed = [&](int w, int k, double* ms) -> int {
         int r = fgpe_batch_config(b, w, k);
         if (r) return r;
@@ -1647,7 +1679,7 @@ int fgpe_batch_autotune(fgpe_batch_t* b, int trial_steps, const char* cache_path
             for (int i = 0; i < n; ++i)
                 if (sizes[i] == classes[ci]) fgpe_set_kernels(b->inst[i], opt ? FGPE_KERNELS_GENERIC : FGPE_KERNELS_AUTO);
             int r = timed(std::min(n, 64), 8, &tms[opt]);
-            if (r) return r;
+            if (r) return finish(r);
         }
         const int pick = tms[1] < tms[0] ? 1 : 0;
         fam[ci] = pick ? 'g' : 'f';
@@ -1664,24 +1696,14 @@ int fgpe_batch_autotune(fgpe_batch_t* b, int trial_steps, const char* cache_path
         for (int k : ks) {
             double ms = 0;
             int r = timed(w, k, &ms);
-            if (r) return r;
+            if (r) return finish(r);
             if (ms < best_ms) { best_ms = ms; bw = w; bk = k; }
         }
     }
-    cudaEventDestroy(t0);
-    cudaEventDestroy(t1);
-    // restore the states
-    for (int i = 0; i < n; ++i) {
-        fgpe_t* h = b->inst[i];
-        const size_t bytes = (size_t)h->npts * h->ms * h->cs;
-        BCK(cudaMemcpy(h->S, save[i], bytes, cudaMemcpyDeviceToDevice));
-        BCK(cudaMemcpy(h->psi, (char*)save[i] + bytes, bytes, cudaMemcpyDeviceToDevice));
-        BCK(cudaMemcpy(h->info, save_info[i], 2 * INFO_LEN * sizeof(double), cudaMemcpyDeviceToDevice));
-        h->S_valid = flags[3 * i]; h->psi_valid = flags[3 * i + 1]; h->prev_valid = flags[3 * i + 2];
-        cudaFree(save[i]);
-        cudaFree(save_info[i]);
-    }
-    int r = fgpe_batch_config(b, bw, bk);
+#undef ACK
+    int r = finish(FGPE_OK);
+    if (r) return r;
+    r = fgpe_batch_config(b, bw, bk);
     if (r) return r;
     if (cache_path) {
         FILE* f = fopen(cache_path, "a");
@@ -1908,6 +1930,17 @@ extern "C" int fgpe_checkpoint_load(fgpe_t* h, const char* path, long long* step
     if (p.dim != h->p.dim || p.spin != h->p.spin || p.nx != h->p.nx || p.ny != h->p.ny || p.nz != h->p.nz ||
         p.precision != h->p.precision)
         return fail(h, FGPE_E_ARG, "checkpoint grid, spin or precision differs from the handle's");
+    // a resume continues bit-identically only under the same physics: the
+    // spacings, time step, time mode, couplings, trap and MAG must match too
+    {
+        bool same = p.dx == h->p.dx && p.dy == h->p.dy && p.dz == h->p.dz && p.dt == h->p.dt &&
+                    p.imag_time == h->p.imag_time && p.mag == h->p.mag;
+        for (int i = 0; i < 3; ++i)
+            same = same && p.tau[i] == h->p.tau[i] && p.gamma[i] == h->p.gamma[i] && p.alpha[i] == h->p.alpha[i];
+        if (!same)
+            return fail(h, FGPE_E_ARG,
+                        "checkpoint parameters (spacings, DT, time mode, TAU, GAMMA, ALPHA or MAG) differ from the handle's");
+    }
     const size_t want = head + ((flags & 1) ? bytes : 0) + ((flags & 2) ? bytes : 0) + 8;
     if (all.size() != want || !(flags & 3)) return fail(h, FGPE_E_ARG, std::string(path) + ": truncated or malformed");
     if (flags & 1) { CK(cudaMemcpyAsync(h->psi, &all[o], bytes, cudaMemcpyHostToDevice, h->st)); o += bytes; }
@@ -1927,9 +1960,12 @@ extern "C" int fgpe_checkpoint_load(fgpe_t* h, const char* path, long long* step
 // ===================================================== NORMC without allocation
 // fgpe_normc_noalloc: NORMC of a caller's device-resident spinor with no
 // handle and no allocation of any kind.  Its only scratch is the file-scope
-// array below (per-line Simpson integrals plus the last-block counter).  The
-// address is looked up once per device with that device current, on the
-// first call made there; afterwards a call only launches one kernel.
+// array below (per-line Simpson integrals plus the last-block counter).  Its
+// device address is looked up on every call, in the context current at the
+// call: the first call in a context loads the module there (the set-up
+// step), later lookups only read the runtime's symbol table and synchronise
+// nothing.  So a context created after cudaDeviceReset, or a caller's own
+// non-primary context, gets its own scratch rather than a stale address.
 // The counter must be zero when a call starts: it is zero when the module is
 // loaded and the last block of every call sets it back to zero.  The line
 // values need no initial contents (every call writes all it reads).  Two calls
@@ -2006,9 +2042,6 @@ k_normc_noalloc(const double2* __restrict__ phi, int nx, int ny, long long nline
     if (threadIdx.x == 0) s->counter = 0u;
 }
 
-std::mutex g_noalloc_mu;
-NoAllocScratch* g_noalloc_ptr[64] = {};
-
 }  // namespace
 
 extern "C" int fgpe_normc_noalloc(int dim, int spin, int nx, int ny, int nz, double dx, double dy, double dz,
@@ -2030,21 +2063,9 @@ extern "C" int fgpe_normc_noalloc(int dim, int spin, int nx, int ny, int nz, dou
         return fail(nullptr, FGPE_E_ARG,
                     "grid too large for the static scratch: (ny*nz lines) x components = " +
                         std::to_string(nlines * ms) + " exceeds " + std::to_string(kNoAllocMaxValues));
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return fail(nullptr, FGPE_E_CUDA, cudaGetErrorString(e));
-    if (dev < 0 || dev >= 64) return fail(nullptr, FGPE_E_ARG, "device ordinal beyond 63");
     NoAllocScratch* s = nullptr;
-    {
-        std::lock_guard<std::mutex> lock(g_noalloc_mu);
-        if (!g_noalloc_ptr[dev]) {
-            void* p = nullptr;
-            e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-            if (e != cudaSuccess) return fail(nullptr, FGPE_E_CUDA, std::string("scratch lookup: ") + cudaGetErrorString(e));
-            g_noalloc_ptr[dev] = (NoAllocScratch*)p;
-        }
-        s = g_noalloc_ptr[dev];
-    }
+    cudaError_t e = cudaGetSymbolAddress((void**)&s, g_noalloc_scratch);
+    if (e != cudaSuccess) return fail(nullptr, FGPE_E_CUDA, std::string("scratch lookup: ") + cudaGetErrorString(e));
     const long long npts = nlines * nx;
     const unsigned grid = (unsigned)std::min<long long>((nlines + 7) / 8, 148LL * 8);
     cudaStream_t st = (cudaStream_t)stream;

@@ -377,8 +377,9 @@ __global__ void __launch_bounds__(TH, FGPE_COL_MINB) k_col_fast(StepConst c, Col
             for (int p = threadIdx.x; p < N * TX; p += TH) {
                 const int t = p % TX, e = p / TX;
                 const int ix = c.fx[x0 + t];
+                // y lines: ky at the line position; z lines: ky at the tile's y
                 int iy, iz;
-                if (c.dim == 2) { iy = c.fy[e]; iz = 0; } else { iy = c.fy[oth]; iz = c.fz[e]; }
+                if (a.axis == 1) { iy = c.fy[e]; iz = 0; } else { iy = c.fy[oth]; iz = c.fz[e]; }
                 cx<T> v[MS];
 #pragma unroll
                 for (int m = 0; m < MS; ++m) v[m] = cur[(m * LPN + e + (e >> 3)) * TX + t];
@@ -386,8 +387,8 @@ __global__ void __launch_bounds__(TH, FGPE_COL_MINB) k_col_fast(StepConst c, Col
 #pragma unroll
                     for (int m = 0; m < MS; ++m) v[m] = cscale(v[m], fac[m]);
                 }
-                apply_ke<T, MS>(c, ix, iy, iz, v);
-                apply_soc<T, MS>(c, c.kx[ix], c.dim >= 2 ? c.ky[iy] : 0.0, v);
+                if (a.flags & COL_KE) apply_ke<T, MS>(c, ix, iy, iz, v);
+                if (a.flags & COL_SOC) apply_soc<T, MS>(c, c.kx[ix], c.ky[iy], v);
 #pragma unroll
                 for (int m = 0; m < MS; ++m) cur[(m * LPN + e + (e >> 3)) * TX + t] = v[m];
             }

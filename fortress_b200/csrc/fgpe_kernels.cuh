@@ -205,13 +205,14 @@ k_col(StepConst c, ColArgs a) {
         for (int p = threadIdx.x; p < n * TX; p += blockDim.x) {
             const int t = p % TX, e = p / TX;
             const int ix = c.fx[x0 + t];
+            // y lines: ky at the line position; z lines: ky at the block's y
             int iy, iz;
-            if (c.dim == 2) { iy = c.fy[e]; iz = 0; } else { iy = c.fy[blockIdx.y]; iz = c.fz[e]; }
+            if (a.axis == 1) { iy = c.fy[e]; iz = 0; } else { iy = c.fy[blockIdx.y]; iz = c.fz[e]; }
             cx<T> v[MS];
 #pragma unroll
             for (int m = 0; m < MS; ++m) v[m] = sm[(m * lpn + pad_idx(e)) * TX + t];
-            apply_ke<T, MS>(c, ix, iy, iz, v);
-            apply_soc<T, MS>(c, c.kx[ix], c.dim >= 2 ? c.ky[iy] : 0.0, v);
+            if (a.flags & COL_KE) apply_ke<T, MS>(c, ix, iy, iz, v);
+            if (a.flags & COL_SOC) apply_soc<T, MS>(c, c.kx[ix], c.ky[iy], v);
 #pragma unroll
             for (int m = 0; m < MS; ++m) sm[(m * lpn + pad_idx(e)) * TX + t] = v[m];
         }

@@ -21,7 +21,12 @@ enum {
 };
 
 enum { ROW_FULL = 0, ROW_FWD = 1, ROW_INV = 2 };
-enum { COL_SCALE = 1, COL_FWD = 2, COL_KOP = 4, COL_INV = 8 };
+// Column-pass work: COL_KE and COL_SOC act in k-space between the forward
+// and inverse transforms of the pass.  In 3D the SO-coupling factor depends
+// on (kx, ky) only, so it commutes with the z transform and runs in the
+// inverse y pass, after the z pass has applied KE (cgpe3d.f90:452-454 keep
+// the order KE then SOC).
+enum { COL_SCALE = 1, COL_FWD = 2, COL_KE = 4, COL_INV = 8, COL_SOC = 16, COL_KOP = COL_KE | COL_SOC };
 enum { OBS_FULL = 0, OBS_NORMS = 1, OBS_NORMALIZE = 2 };
 enum { OP_KE = 1, OP_SOC = 2, OP_SE = 3, OP_SP = 4, OP_SCALE = 5 };
 
@@ -45,6 +50,7 @@ struct ColArgs {
     long long axis_stride, other_stride;
     int n, tx, flags;
     int n_other;       // number of positions along the third axis (1 in 2D)
+    int axis;          // transformed axis: 1 (y) or 2 (z)
 };
 
 // Long 1D lines, N = N1*N2 points, handled as an N2 x N1 array (x = n1 + N1*n2)

@@ -52,7 +52,9 @@ def run(prop, niter, stp, tol, dt, imag, nstp=0, on_nstp=None):
             en, mu, mz, rms = prop.observables()
             if imag:
                 c = prop.conv() / (stp * 2.0 * dt)
-                ce = abs(en - en_old) / (stp * 2.0 * dt)
+                # EN_OLD starts at 0 and takes EN after every step
+                # (cgpe1d.f90:294, 507): only a boundary at II = 1 sees the 0
+                ce = abs(en - (en_old if ii > 1 else 0.0)) / (stp * 2.0 * dt)
                 res.conv.append([2.0 * ii * dt, c, ce])
                 if c <= tol or ce <= tol:
                     exited = True

@@ -570,7 +570,9 @@ int main() {
                 double dphi = 0;
                 check(fgpe_conv(h, &dphi), h);
                 const double conv = dphi / (STP * 2.0 * DT);
-                const double conv_en = fabs(en - en_old) / (STP * 2.0 * DT);
+                // EN_OLD starts at 0 and takes EN after every step
+                // (cgpe1d.f90:294, 507): only a boundary at II = 1 sees the 0
+                const double conv_en = fabs(en - (ii > 1 ? en_old : 0.0)) / (STP * 2.0 * DT);
                 fprintf(f9, "%s%s%s\n", fList(2.0 * ii * DT).c_str(), fList(conv).c_str(), fList(conv_en).c_str());
                 if (conv <= TOL || conv_en <= TOL) { exited = true; break; }
             }

@@ -216,16 +216,17 @@ int fgpe_checkpoint_load(fgpe_t *h, const char *path, long long *step, double *u
  * memory, such as a host code whose device memory is reserved up front by
  * its own pool or a solver that must not synchronise the device in the
  * middle of a run (cudaMalloc/cudaFree synchronise).  No counterpart in the
- * reference (NORMC, cgpe1d.f90:957-993, works on its module state).
+ * reference.
  *   phi_dev: complex128, the PHI layout of fgpe_set_state; norm_dev: 2*spin+1
  *   doubles of device memory; stream: cudaStream_t (NULL = legacy default).
  * Asynchronous: the result is in norm_dev once the stream reaches it.
  * Limits: every used axis an even number >= 8 of points (the reference's
  * Simpson rule), and (ny*nz lines) x (2*spin+1) <= 262144, the size of the
- * library's fixed 2 MiB scratch; larger grids return FGPE_E_ARG.  The first
- * call on each device looks the scratch up (cudaGetSymbolAddress) with that
- * device current; make it before any stream capture.  Calls on one device
- * share the scratch: never have two in flight at once. */
+ * library's fixed 2 MiB scratch; larger grids return FGPE_E_ARG.  Every call
+ * looks the scratch up (cudaGetSymbolAddress) in the context current at the
+ * call; the first call in a context also loads the library's device code
+ * there, so make it before any stream capture.  Calls on one device share
+ * the scratch: never have two in flight at once. */
 int fgpe_normc_noalloc(int dim, int spin, int nx, int ny, int nz, double dx, double dy, double dz,
                        const void *phi_dev, double *norm_dev, void *stream);
 
@@ -233,6 +234,12 @@ int fgpe_normc_noalloc(int dim, int spin, int nx, int ny, int nz, double dx, dou
 int fgpe_version(void);
 int fgpe_device_ok(void);                /* 1 if an sm_100 device is usable */
 int fgpe_kernel_launches(fgpe_t *h, long long *count);  /* kernels launched */
+/* FP64 FMA throughput of the current device in TFLOP/s (2 flops per FMA),
+ * from a CUDA-event-timed launch of independent FMA chains on every SM: the
+ * compute-roofline denominator of the step kernels, whose exponentials,
+ * spin-2 matrix products and FFT butterflies run on the FP64 pipe.  No
+ * counterpart in the reference (a measurement aid). */
+int fgpe_fp64_fma_rate(int iters, double *tflops);
 
 #ifdef __cplusplus
 }

@@ -1,5 +1,7 @@
 """bench.py's reference arm on the CPU: one JSON line with the keys the
-benchmark contract asks for, from rank 0 only."""
+benchmark contract asks for, from rank 0 only, on the q2D workload (the 256^3
+default takes minutes of oracle time per step on a small host); and both
+arms of the default workload build the same config and initial state."""
 import json
 import os
 import subprocess
@@ -11,7 +13,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 def _run(env_extra):
     env = dict(os.environ, OMP_NUM_THREADS="4", **env_extra)
     r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
-                        "--steps", "1", "--warmup", "3"],
+                        "--workload", "q2d", "--steps", "1", "--warmup", "3"],
                        cwd=ROOT, env=env, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     return [l for l in r.stdout.splitlines() if l.startswith("{")]
@@ -37,3 +39,18 @@ def test_reference_arm_prints_one_contract_line():
 
 def test_reference_arm_other_ranks_print_nothing():
     assert _run({"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"}) == []
+
+
+def test_both_arms_share_config_and_state():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("bench_mod", os.path.join(ROOT, "bench.py"))
+    b = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(b)
+    w = b.D3
+    assert b.bench_config(w, "fp64", 1) == b.bench_config(w, "fp64", 1, impl="reference")
+    assert b.bench_config(w)["workload"] == "3d-spin1-SO-imag-256^3"
+    assert b.bench_config(w)["grid"] == [256, 256, 256]
+    # the seeded start is reproducible (both arms build it the same way)
+    n, d = (16, 16, 16), (1.6, 1.6, 1.6)
+    a, c = b.initial_state(w, n, d), b.initial_state(w, n, d)
+    assert a.shape == (16, 16, 16, 3) and (a == c).all()

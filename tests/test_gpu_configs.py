@@ -1,0 +1,223 @@
+"""Parity with the oracle at the benchmark configurations' own parameters.
+
+* q1D spin-1 SO-coupled imaginary-time ground state (NX=1024, DX=0.05,
+  DT=5e-4, mass 23, a0/a2 = 50/55.01 a_B, NATOMS=10000, NU=(20,400,400),
+  GAMMAX=0.5, TOL=1e-10, NITER=20000, STP=100) run through the reference's
+  time loop to its exit on the GPU and on the oracle (cgpe1d.f90:433-519,
+  exit test 480-487).
+* q2D spin-2 real-time quench (512^2, DT=1e-4, Rb-87 a0/a2/a4 =
+  87.93/91.28/99.18, NATOMS=50000, NU=(20,20,500), GAMMAX 1.0 -> 1.2) from
+  the imaginary-time ground state plus seeded noise: 2000 steps at 512^2 and
+  all 50 000 steps on a 128^2 grid of the same box (cgpe2d.f90:440-531).
+* Instances of the phase-diagram sweep box (q2D spin-1, DX=0.1, DT=5e-4,
+  gamma in [0,2]^2, c0 in [100,2000], c2/c0 in [-0.05,0.05], NUY/NUX in
+  [1,2]) including the 384^2 and 512^2 sizes, advanced by the batched
+  launcher in FP64 and in FP32 and compared instance by instance with the
+  oracle.
+
+Bars: energy, chemical potentials and rms sizes within 1e-10 relative and
+densities within 1e-9 max-abs for FP64; FP32-bulk errors against the oracle
+are reported and held to the bounds written beside them.
+"""
+import json
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests.helpers import oracle_kwargs
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    a, b = np.asarray(a, float), np.asarray(b, float)
+    return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-300)))
+
+
+# ------------------------------------------------------------------ config 1
+def _config1():
+    from fortress_b200.config import RunConfig
+    return RunConfig(dim=1, spin=1, niter=20000, stp=100, nstp=20000, n=(1024, 1, 1), d=(0.05, 1.0, 1.0),
+                     dt=5e-4, mass=23.0, a=(50.0, 55.01, 0.0), natoms=10000, nu=(20.0, 400.0, 400.0),
+                     tol=1e-10, switch_im=1, gamma=(0.5, 0.0, 0.0))
+
+
+def _config1_state(cfg):
+    """exp(-x^2/2)/pi^(1/4) in each component times (1 + 1e-3 u), u ~ U[0,1)
+    (PCG64 seed 1); the loop's initial NORMT normalises it to 1."""
+    n, d = cfg.n[0], cfg.d[0]
+    x = (-1.0 + 2.0 * np.arange(n) / n) * n * d / 2.0
+    g = np.exp(-x * x / 2.0) / np.pi ** 0.25
+    rng = np.random.default_rng(1)
+    return np.stack([g * (1.0 + 1e-3 * rng.uniform(size=n)) for _ in range(3)], axis=-1).astype(complex)
+
+
+def test_config1_q1d_spin1_ground_state_to_exit():
+    import fortress_b200 as F
+    from fortress_b200.driver import run
+    cfg = _config1()
+    p = cfg.params("fp64")
+    phi = _config1_state(cfg)
+    orc = O.Oracle(**oracle_kwargs(p))
+    orc.set_state(phi)
+    ro = O.run_loop(orc, cfg.niter, cfg.stp, cfg.tol, cfg.dt, 1)
+    prop = F.Propagator(**p)
+    try:
+        prop.set_state(phi)
+        rg = run(prop, cfg.niter, cfg.stp, cfg.tol, cfg.dt, 1)
+        dens_g = np.abs(prop.state()) ** 2
+    finally:
+        prop.close()
+    dens_o = np.abs(orc.state()) ** 2
+    fo, fg = ro["final"], rg.final
+    # same exit iteration and the same convergence rows along the way
+    assert fg["ii_minus_1"] == fo["ii_minus_1"]
+    assert len(rg.conv) == len(ro["conv"])
+    # CONV is a one-step difference of nearly equal states divided by
+    # STP*2*DT: state agreement of ~1e-14 shows up as ~1e-13 here
+    for a, b in zip(rg.conv, ro["conv"]):
+        assert a[0] == b[0]
+        assert abs(a[1] - b[1]) <= 1e-11 + 1e-6 * abs(b[1])
+    assert _rel(fg["en"], fo["en"]) <= 1e-10
+    assert _rel(fg["mu"], fo["mu"]) <= 1e-10
+    assert _rel(fg["rms"], fo["rms"]) <= 1e-10
+    assert np.abs(dens_g - dens_o).max() <= 1e-9
+    for a, b in zip(rg.file2, ro["file2"]):
+        assert a[0] == b[0] and _rel(a[1:], b[1:]) <= 1e-10
+    print(json.dumps({"config1": {"exit_ii_minus_1": fg["ii_minus_1"], "en_rel": _rel(fg["en"], fo["en"]),
+                                  "density_maxabs": float(np.abs(dens_g - dens_o).max())}}))
+
+
+# ------------------------------------------------------------------ config 2
+def _q2d(n, gamma, imag=False, dt=1e-4):
+    from fortress_b200.config import RunConfig
+    c = RunConfig(dim=2, spin=2, n=(n, n, 1), d=(25.6 / n, 25.6 / n, 1.0), dt=dt, mass=87.0,
+                  a=(87.93, 91.28, 99.18), natoms=50000, nu=(20.0, 20.0, 500.0), switch_im=int(imag),
+                  gamma=(gamma[0], gamma[1], 0.0))
+    return c.params("fp64")
+
+
+def _quench_start(F, n, seed=2):
+    """Ground state at gamma = (1, 1) (3000 imaginary-time steps of 1e-3 from
+    INITIALIZE's spin-2 guess) plus 1e-3 of the peak in seeded complex
+    Gaussian noise."""
+    p = _q2d(n, (1.0, 1.0), imag=True, dt=1e-3)
+    d = p["d"][0]
+    x = (-1.0 + 2.0 * np.arange(n) / n) * n * d / 2.0
+    g = np.sqrt(0.2) * np.exp(-(x[:, None] ** 2 + x[None, :] ** 2) / 2.0) / np.sqrt(np.pi)
+    r = F.Propagator(**p)
+    try:
+        r.set_state(np.repeat(g[:, :, None, None], 5, axis=3).astype(complex))
+        r.normt()
+        r.step(3000)
+        phi = r.state()
+    finally:
+        r.close()
+    rng = np.random.default_rng(seed)
+    return phi + 1e-3 * np.abs(phi).max() * (rng.standard_normal(phi.shape) + 1j * rng.standard_normal(phi.shape))
+
+
+def _quench_compare(n, steps, tol_e, tol_d):
+    import fortress_b200 as F
+    phi = _quench_start(F, n)
+    p = _q2d(n, (1.2, 1.0))
+    orc = O.Oracle(**oracle_kwargs(p))
+    orc.set_state(phi)
+    prop = F.Propagator(**p)
+    try:
+        prop.set_state(phi)
+        prop.step(steps)                 # enqueued: the GPU runs while the oracle does
+        orc.step(steps)
+        en_g, mu_g, mz_g, rms_g = prop.observables()
+        dens_g = np.abs(prop.state()) ** 2
+    finally:
+        prop.close()
+    en_o, mu_o, mz_o = orc.energy()
+    dens_o = np.abs(orc.state()) ** 2
+    out = {"grid": n, "steps": steps, "en_rel": _rel(en_g, en_o), "mu_rel": _rel(mu_g, mu_o),
+           "rms_rel": _rel(rms_g, orc.rad()), "density_maxabs": float(np.abs(dens_g - dens_o).max())}
+    print(json.dumps({"config2": out}))
+    assert out["en_rel"] <= tol_e and out["mu_rel"] <= tol_e and out["rms_rel"] <= tol_e
+    assert out["density_maxabs"] <= tol_d
+
+
+def test_config2_quench_512_2000_steps():
+    _quench_compare(512, 2000, 1e-10, 1e-9)
+
+
+def test_config2_quench_128_all_50000_steps():
+    _quench_compare(128, 50000, 1e-10, 1e-9)
+
+
+# ------------------------------------------------------------------ config 4
+def _sweep_instances(count, seed=4, precision="fp64", force_sizes=()):
+    """Seeded draws from the sweep box (the bench's phase-diagram sweep
+    uses the same box); force_sizes replaces the first sizes drawn."""
+    rng = np.random.default_rng(seed)
+    sizes = list(rng.choice([128, 192, 256, 384, 512], size=count))
+    for k, s in enumerate(force_sizes):
+        sizes[k] = s
+    out = []
+    for k in range(count):
+        g = rng.uniform(0, 2, 2)
+        c0 = rng.uniform(100, 2000)
+        c2 = c0 * rng.uniform(-0.05, 0.05)
+        ay = rng.uniform(1, 2)
+        n = int(sizes[k])
+        out.append(dict(dim=2, spin=1, n=(n, n), d=(0.1, 0.1), dt=5e-4, imag_time=True,
+                        tau=(2 * c0, 2 * c2, 0.0), gamma=(float(g[0]), float(g[1])), alpha=(1.0, ay, 1.0),
+                        precision=precision))
+    return out
+
+
+def _sweep_guess(p, seed):
+    n, d = p["n"][0], p["d"][0]
+    x = (-1.0 + 2.0 * np.arange(n) / n) * n * d / 2.0
+    ay = p["alpha"][1]
+    g = np.exp(-(x[:, None] ** 2 + ay * x[None, :] ** 2) / 2.0) / np.sqrt(np.pi)
+    rng = np.random.default_rng(seed)
+    return np.stack([g * (1.0 + 1e-3 * rng.uniform(size=g.shape)) for _ in range(3)], axis=-1)[:, :, None, :] \
+        .astype(complex)
+
+
+def test_config4_sweep_instances_fp64_and_fp32_vs_oracle():
+    from fortress_b200.batch import Batch
+    steps = 300
+    p64 = _sweep_instances(8, force_sizes=(512, 384))
+    assert {512, 384} <= {p["n"][0] for p in p64}
+    p32 = [dict(p, precision="fp32") for p in p64]
+    states = [_sweep_guess(p, 40 + i) for i, p in enumerate(p64)]
+    b64, b32 = Batch(p64), Batch(p32)
+    for i, phi in enumerate(states):
+        for b in (b64, b32):
+            b[i].set_state(phi)
+            b[i].normt()
+    b64.step(steps)
+    b32.step(steps)
+    worst32 = {"en": 0.0, "mu": 0.0, "rms": 0.0, "dens": 0.0}
+    for i, p in enumerate(p64):
+        q = dict(p)
+        q.pop("precision")
+        orc = O.Oracle(**oracle_kwargs(q))
+        orc.set_state(states[i])
+        orc.normt()
+        orc.step(steps)
+        en_o, mu_o, _ = orc.energy()
+        rms_o = orc.rad()
+        dens_o = np.abs(orc.state()) ** 2
+        en, mu, mz, rms = b64[i].observables()
+        assert _rel(en, en_o) <= 1e-10, (i, p["n"])
+        assert _rel(mu, mu_o) <= 1e-10 and _rel(rms, rms_o) <= 1e-10, (i, p["n"])
+        assert np.abs(np.abs(b64[i].state()) ** 2 - dens_o).max() <= 1e-9, (i, p["n"])
+        en, mu, mz, rms = b32[i].observables()
+        worst32["en"] = max(worst32["en"], _rel(en, en_o))
+        worst32["mu"] = max(worst32["mu"], _rel(mu, mu_o))
+        worst32["rms"] = max(worst32["rms"], _rel(rms, rms_o))
+        worst32["dens"] = max(worst32["dens"],
+                              float(np.abs(np.abs(b32[i].state()) ** 2 - dens_o).max() / dens_o.max()))
+    print(json.dumps({"config4_fp32_vs_oracle_worst": worst32, "steps": steps}))
+    # FP32 bulk against the FP64 oracle after 300 imaginary-time steps
+    # (relative; densities relative to their peak)
+    assert worst32["en"] <= 1e-5 and worst32["mu"] <= 1e-5
+    assert worst32["rms"] <= 1e-4 and worst32["dens"] <= 1e-4
