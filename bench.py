@@ -275,6 +275,8 @@ def capture(args):
         assert np.isfinite(en)
         print(json.dumps({"capture": "golden-1d-spin2-2048", "steps": args.warmup + args.steps, "en": en}))
         return
+    if args.workload == "tour":
+        return kernel_tour(args)
     w = WORKLOADS[args.workload]
     if w is D3:
         g = args.grid or 192
@@ -294,6 +296,69 @@ def capture(args):
     assert np.all(np.isfinite(nrm))
     print(json.dumps({"capture": w["name"], "grid": list(n[:w["dim"]]), "precision": args.precision,
                       "steps": args.warmup + args.steps, "norm": float(nrm.sum())}))
+
+
+def kernel_tour(args):
+    """Every kernel family of the library once, each on a small case, for a
+    per-kernel ncu capture (ncu -k regex:... -c <launches>): the observables
+    (k_obs), state import/export (k_import, k_export), the NORMC read-back
+    (k_norms_out), the 1D kernels (k_1d single block, k_cl1d cluster, k_r1d /
+    k_c1d split), the generic row/column kernels (k_row, k_col on 160-point
+    lines), the unfused operators (k_pointwise_op, k_permute), the
+    handle-free NORMC (k_normc_noalloc) and the learned-guess kernels (GEMM,
+    bias/GELU, dense tcgen05 layer, MSE, Adam)."""
+    import ctypes
+    import numpy as np
+    import torch
+    import fortress_b200 as F
+    from fortress_b200 import _abi
+    rng = np.random.default_rng(0)
+
+    def rnd(shape):
+        return (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)) * 0.1
+
+    # 3D 192^3 spin-1: import (FP32 handle), observables, export, NORMC read-back
+    cfg = run_config(D3, (192, 192, 192), (25.6 / 192,) * 3)
+    prop = F.Propagator(**cfg.params("fp32"))
+    prop.set_state(initial_state(D3, (192, 192, 192), (25.6 / 192,) * 3))
+    prop.normt()
+    prop.step(2)
+    prop.observables()
+    pinned = torch.empty(8, dtype=torch.float64, pin_memory=True)
+    prop.norms_async(pinned.data_ptr())
+    prop.state()
+    prop.close()
+    # 1D: single block (spin-1, 256), cluster (spin-2, 2048), split (spin-2, 8192)
+    for n, spin, d in ((256, 1, 0.1), (2048, 2, 0.05), (8192, 2, 0.02)):
+        q = F.Propagator(dim=1, spin=spin, n=(n,), d=(d,), dt=1e-4, imag_time=True,
+                         tau=(200.0, 5.0, -3.0), gamma=(0.5,), alpha=(1.0, 20.0, 20.0))
+        x = (-1.0 + 2.0 * np.arange(n) / n) * n * d / 2.0
+        q.set_state(np.repeat(np.exp(-x * x / 2)[:, None], 2 * spin + 1, axis=1).astype(complex))
+        q.step(3)
+        q.close()
+    # generic 2D kernels (160-point lines) and the unfused operators
+    q = F.Propagator(dim=2, spin=2, n=(160, 160), d=(0.15, 0.15), dt=1e-4, imag_time=False,
+                     tau=(300.0, 10.0, -8.0), gamma=(0.5, 0.3), alpha=(1.0, 1.2, 1.0))
+    q.set_state(rnd((160, 160, 5)))
+    q.step(3)
+    for op in ("FFT", "KE", "SOC", "BFT", "SE", "SP"):
+        q.apply_op(op)
+    q.close()
+    # handle-free NORMC
+    phi = torch.tensor(rnd((3, 128, 128)).astype(np.complex128), device="cuda")
+    out = torch.zeros(3, dtype=torch.float64, device="cuda")
+    rc = _abi.load().fgpe_normc_noalloc(2, 1, 128, 128, 1, 0.1, 0.1, 0.1, ctypes.c_void_p(phi.data_ptr()),
+                                        ctypes.c_void_p(out.data_ptr()), None)
+    assert rc == 0
+    # learned-guess kernels: one training step at 64^2, batch 16
+    from fortress_b200 import fno as FN
+    net = FN.FNO(64, 16, seed=7)
+    a = FN.input_channels(rng.uniform(-1, 1, (16, 5)), 64)
+    tgt = torch.randn(6, 16 * 64 * 64, device="cuda", generator=torch.Generator("cuda").manual_seed(1))
+    net.forward(a); net.loss(tgt); net.backward(); net.adam()
+    torch.cuda.synchronize()
+    assert not net.tc_error()
+    print(json.dumps({"capture": "kernel-tour"}))
 
 
 def kernel_pass(prop, flush, steps):
@@ -637,11 +702,12 @@ def main():
                     help="arithmetic of the headline value (default fp64; the fp32 figure is added beside it)")
     ap.add_argument("--no-fp32", action="store_true", help="skip the FP32-bulk figure")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="3d", choices=["3d", "q2d", "sweep", "golden1d", "fno"],
+    ap.add_argument("--workload", default="3d", choices=["3d", "q2d", "sweep", "golden1d", "fno", "tour"],
                     help="3d: 256^3 spin-1 imaginary time (headline); q2d: 512^2 spin-2 real-time quench; "
                          "sweep: 512 ragged q2D spin-1 instances in one batched graph launch; "
                          "golden1d: the reference's published run (1D spin-2, 2048 points, to convergence); "
-                         "fno: with --capture only, learned-guess training steps")
+                         "fno: with --capture only, learned-guess training steps; "
+                         "tour: with --capture only, every kernel family once")
     ap.add_argument("--capture", action="store_true",
                     help="run only the workload's step kernels (warmup + steps launches of each, no timing, "
                          "no other work) for profiler captures")
@@ -653,8 +719,8 @@ def main():
     args.precision = args.precision or "fp64"
     if args.capture:
         return capture(args)
-    if args.workload == "fno":
-        ap.error("--workload fno is a profiling case: use it with --capture")
+    if args.workload in ("fno", "tour"):
+        ap.error(f"--workload {args.workload} is a profiling case: use it with --capture")
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

@@ -25,6 +25,8 @@ FGPE_FP64 = 0
 FGPE_FP32 = 1
 FGPE_STEP_DEFAULT = 0
 FGPE_STEP_NO_SNAPSHOT = 1
+FGPE_BATCH_BRANCHES = 0
+FGPE_BATCH_GROUPED = 1
 
 OPS = {"FFT": 1, "KE": 2, "SOC": 3, "BFT": 4, "SE": 5, "SP": 6}
 
@@ -39,7 +41,7 @@ EXPORTS = (
     "fgpe_batch_last_error", "fgpe_batch_config", "fgpe_batch_step", "fgpe_batch_observables",
     "fgpe_batch_autotune", "fgpe_batch_tuning", "fgpe_set_kernels", "fgpe_normc_noalloc",
     "fgpe_checkpoint_save", "fgpe_checkpoint_load", "fgpe_batch_step_timed", "fgpe_norms_sink",
-    "fgpe_fp64_fma_rate",
+    "fgpe_fp64_fma_rate", "fgpe_batch_mode",
 )
 
 
@@ -112,6 +114,7 @@ def load():
         "fgpe_checkpoint_save": ([vp, ctypes.c_char_p, ctypes.c_longlong, dp], ip),
         "fgpe_checkpoint_load": ([vp, ctypes.c_char_p, ctypes.POINTER(ctypes.c_longlong), dp], ip),
         "fgpe_fp64_fma_rate": ([ip, dp], ip),
+        "fgpe_batch_mode": ([vp, ip], ip),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

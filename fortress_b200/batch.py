@@ -54,6 +54,13 @@ class Batch:
     def config(self, width=0, steps_per_graph=0):
         check_batch(self._L.fgpe_batch_config(self._b, int(width), int(steps_per_graph)), self._b)
 
+    def mode(self, grouped):
+        """grouped=True: instances sharing a q2D grid shape advance together,
+        one column-pass and one row-pass launch per step per group
+        (fgpe_batch_mode); False: one graph branch per instance."""
+        m = _abi.FGPE_BATCH_GROUPED if grouped else _abi.FGPE_BATCH_BRANCHES
+        check_batch(self._L.fgpe_batch_mode(self._b, m), self._b)
+
     def tuning(self):
         w, k = ctypes.c_int(), ctypes.c_int()
         check_batch(self._L.fgpe_batch_tuning(self._b, ctypes.byref(w), ctypes.byref(k)), self._b)

@@ -20,6 +20,7 @@
 #include "../../include/fgpe.h"
 #include "fgpe_kernels.cuh"
 #include "fgpe_fast.cuh"
+#include "fgpe_group.cuh"
 #include "fno_kernels.cuh"
 #include "../../include/fno.h"
 
@@ -1341,8 +1342,23 @@ int fgpe_debug_align_fault(unsigned long long* out4) {
 // ================================================================ batches
 }  // extern "C"
 
+// One group of the grouped batch mode: instances of one q2D grid shape,
+// spin and precision whose passes run as shared launches (fgpe_group.cuh).
+struct BatchGroup {
+    int nx = 0, ny = 0, ms = 0, fp32 = 0;
+    std::vector<int> members;
+    InstDesc* d_desc = nullptr;      // per-instance descriptors (device)
+    InstDesc* h_desc = nullptr;      // pinned staging of the descriptors
+    double* part = nullptr;          // NORMC chunk partials [members][chunks][MS]
+    unsigned* counter = nullptr;     // per-instance chunk counters
+    int row_tiles = 0, chunk = 0, col_tiles = 0, row_grid = 0, col_grid = 0;
+};
+
 struct fgpe_batch_s {
     std::vector<fgpe_t*> inst;
+    int mode = FGPE_BATCH_BRANCHES;
+    std::vector<BatchGroup> groups;         // grouped mode: instances sharing launches
+    std::vector<int> loose;                 // grouped mode: instances on their own branches
     cudaStream_t origin = nullptr;
     std::vector<cudaStream_t> lanes;
     std::vector<cudaEvent_t> ev;            // fork/join events, one per lane + 1
@@ -1425,6 +1441,195 @@ int capture(fgpe_batch_t* b, int nsteps) {
     b->exec_steps = nsteps;
     return FGPE_OK;
 }
+// ----------------------------------------------------------- grouped mode
+constexpr int group_chunk(int tiles) {
+    int c = 1;
+    for (int d = 1; d <= 16; ++d) if (tiles % d == 0) c = d;
+    return c;
+}
+template <typename T, int MS, int NX> int setup_group_row(BatchGroup& g) {
+    constexpr int R = row_r(NX), TH = row_th<T, MS, NX>();
+    if (g.ny % R) return FGPE_E_ARG;
+    g.row_tiles = g.ny / R;
+    g.chunk = group_chunk(g.row_tiles);
+    const size_t smem = (size_t)FGPE_ROW_NBUF * MS * R * cpad(NX) * sizeof(cx<T>);
+    g.row_grid = grid_for(k_row_group<T, MS, NX, R, TH>, TH, smem, (int)g.members.size() * (g.row_tiles / g.chunk));
+    return g.row_grid > 0 ? FGPE_OK : FGPE_E_CUDA;
+}
+template <typename T, int MS, int NY> int setup_group_col(BatchGroup& g) {
+    constexpr int TX = col_tx<T>(), TH = col_th<T, MS, NY>();
+    if (g.nx % TX) return FGPE_E_ARG;
+    g.col_tiles = g.nx / TX;
+    const size_t smem = (size_t)MS * cpad(NY) * TX * sizeof(cx<T>);
+    g.col_grid = grid_for(k_col_group<T, MS, NY, TX, TH>, TH, smem, (int)g.members.size() * g.col_tiles);
+    return g.col_grid > 0 ? FGPE_OK : FGPE_E_CUDA;
+}
+template <typename T, int MS, int NX> void launch_group_row(const BatchGroup& g, int snap, cudaStream_t st) {
+    constexpr int R = row_r(NX), TH = row_th<T, MS, NX>();
+    const size_t smem = (size_t)FGPE_ROW_NBUF * MS * R * cpad(NX) * sizeof(cx<T>);
+    GroupArgs a{g.d_desc, (int)g.members.size(), g.row_tiles, g.chunk, snap};
+    k_row_group<T, MS, NX, R, TH><<<g.row_grid, TH, smem, st>>>(a);
+}
+template <typename T, int MS, int NY> void launch_group_col(const BatchGroup& g, cudaStream_t st) {
+    constexpr int TX = col_tx<T>(), TH = col_th<T, MS, NY>();
+    const size_t smem = (size_t)MS * cpad(NY) * TX * sizeof(cx<T>);
+    GroupArgs a{g.d_desc, (int)g.members.size(), g.col_tiles, 1, 0};
+    k_col_group<T, MS, NY, TX, TH><<<g.col_grid, TH, smem, st>>>(a);
+}
+template <typename T, int MS> int group_setup_tm(BatchGroup& g) {
+    int r = FGPE_E_ARG;
+#define GR(NN) r = setup_group_row<T, MS, NN>(g)
+    FAST_SWITCH(g.nx, GR)
+#undef GR
+    if (r) return r;
+    r = FGPE_E_ARG;
+#define GC(NN) r = setup_group_col<T, MS, NN>(g)
+    FAST_SWITCH(g.ny, GC)
+#undef GC
+    return r;
+}
+template <typename T, int MS> void group_launch_tm(const BatchGroup& g, int snap, cudaStream_t st) {
+#define GC(NN) launch_group_col<T, MS, NN>(g, st)
+    FAST_SWITCH(g.ny, GC)
+#undef GC
+#define GR(NN) launch_group_row<T, MS, NN>(g, snap, st)
+    FAST_SWITCH(g.nx, GR)
+#undef GR
+}
+int group_setup(BatchGroup& g) {
+    if (g.fp32) return g.ms == 3 ? group_setup_tm<float, 3>(g) : group_setup_tm<float, 5>(g);
+    return g.ms == 3 ? group_setup_tm<double, 3>(g) : group_setup_tm<double, 5>(g);
+}
+// One whole step of every instance of g: the column pass, then the row pass.
+void group_step(const BatchGroup& g, int snap, cudaStream_t st) {
+    if (g.fp32) { if (g.ms == 3) group_launch_tm<float, 3>(g, snap, st); else group_launch_tm<float, 5>(g, snap, st); }
+    else { if (g.ms == 3) group_launch_tm<double, 3>(g, snap, st); else group_launch_tm<double, 5>(g, snap, st); }
+}
+
+void free_groups(fgpe_batch_t* b) {
+    for (BatchGroup& g : b->groups) {
+        if (g.d_desc) cudaFree(g.d_desc);
+        if (g.h_desc) cudaFreeHost(g.h_desc);
+        if (g.part) cudaFree(g.part);
+        if (g.counter) cudaFree(g.counter);
+    }
+    b->groups.clear();
+    b->loose.clear();
+}
+
+// Sort the instances into groups (q2D, size-specialised kernels on both
+// axes, same grid, spin and precision) and instances that keep their own
+// graph branches; allocate descriptors, NORMC slots and counters.
+int build_groups(fgpe_batch_t* b) {
+    free_groups(b);
+    for (int i = 0; i < (int)b->inst.size(); ++i) {
+        fgpe_t* h = b->inst[i];
+        const bool ok = h->p.dim == 2 && h->fast_row && h->fast_col[1] && fast_size(h->p.nx) && fast_size(h->p.ny);
+        if (!ok) { b->loose.push_back(i); continue; }
+        BatchGroup* g = nullptr;
+        for (BatchGroup& q : b->groups)
+            if (q.nx == h->p.nx && q.ny == h->p.ny && q.ms == h->ms && q.fp32 == h->fp32) g = &q;
+        if (!g) {
+            b->groups.emplace_back();
+            g = &b->groups.back();
+            g->nx = h->p.nx; g->ny = h->p.ny; g->ms = h->ms; g->fp32 = h->fp32;
+        }
+        g->members.push_back(i);
+    }
+    for (BatchGroup& g : b->groups) {
+        int r = group_setup(g);
+        if (r) { free_groups(b); return bfail(b, r, "grouped batch: no launch shape for a group"); }
+        const size_t n = g.members.size();
+        const size_t slots = n * (size_t)(g.row_tiles / g.chunk) * g.ms;
+        BCK(cudaMalloc(&g.d_desc, n * sizeof(InstDesc)));
+        BCK(cudaMallocHost(&g.h_desc, n * sizeof(InstDesc)));
+        BCK(cudaMalloc(&g.part, slots * sizeof(double)));
+        BCK(cudaMalloc(&g.counter, n * sizeof(unsigned)));
+        BCK(cudaMemset(g.counter, 0, n * sizeof(unsigned)));
+    }
+    return FGPE_OK;
+}
+
+// Descriptors from the handles' current buffers and constants (a handle's
+// psi/prev roles and its NORMC sink can change between calls), copied ahead
+// of the graph launch on the batch's launch stream.
+int refresh_descs(fgpe_batch_t* b) {
+    for (BatchGroup& g : b->groups) {
+        const int nci = g.row_tiles / g.chunk;
+        for (size_t k = 0; k < g.members.size(); ++k) {
+            fgpe_t* h = b->inst[g.members[k]];
+            InstDesc& d = g.h_desc[k];
+            d.c = h->sc;
+            d.S = h->S; d.psi = h->psi; d.prev = h->prev;
+            d.info = h->info; d.info_prev = h->info_prev;
+            d.part = g.part + k * (size_t)nci * g.ms;
+            d.counter = g.counter + k;
+        }
+        BCK(cudaMemcpyAsync(g.d_desc, g.h_desc, g.members.size() * sizeof(InstDesc), cudaMemcpyHostToDevice,
+                            b->origin));
+    }
+    return FGPE_OK;
+}
+
+// Grouped mode capture: each group's nsteps as a branch of shared launches
+// (the last two steps write the real-space snapshots of CONV, as a
+// multi-step fgpe_step does), the remaining instances as their own branches.
+int capture_grouped(fgpe_batch_t* b, int nsteps) {
+    drop_graph(b);
+    int r = build_groups(b);
+    if (r) return r;
+    for (fgpe_t* h : b->inst) {
+        if (!h->has_state) return bfail(b, FGPE_E_STATE, "batch instance without a state");
+        if (h->p.dim >= 2 && !h->S_valid) {
+            DISPATCH(h, launch_row, h, ROW_FWD, nullptr);
+            BCK(cudaGetLastError());
+            h->S_valid = true;
+        }
+        BCK(cudaStreamSynchronize(h->st));
+    }
+    const int nbr = (int)b->groups.size() + (int)b->loose.size();
+    r = set_width(b, std::max(b->width, std::min(nbr, 64)));
+    if (r) return r;
+    r = refresh_descs(b);
+    if (r) return r;
+    BCK(cudaStreamSynchronize(b->origin));
+    cudaGraph_t gr;
+    BCK(cudaStreamBeginCapture(b->origin, cudaStreamCaptureModeThreadLocal));
+    BCK(cudaEventRecord(b->ev[0], b->origin));
+    for (int l = 0; l < b->width; ++l) BCK(cudaStreamWaitEvent(b->lanes[l], b->ev[0], 0));
+    int lane = 0;
+    for (const BatchGroup& g : b->groups) {
+        cudaStream_t st = b->lanes[lane++ % b->width];
+        for (int s = 0; s < nsteps; ++s) group_step(g, s == nsteps - 1 ? 1 : (s == nsteps - 2 ? 2 : 0), st);
+        for (int i : g.members) {
+            fgpe_t* h = b->inst[i];
+            h->S_valid = true; h->psi_valid = true; h->prev_valid = true; h->norms_valid = true;
+        }
+    }
+    for (int i : b->loose) {
+        fgpe_t* h = b->inst[i];
+        cudaStream_t keep = h->st;
+        const bool prof = h->prof;
+        h->st = b->lanes[lane++ % b->width];
+        h->prof = false;
+        const int rc = fgpe_step_ex(h, nsteps, FGPE_STEP_DEFAULT);
+        h->st = keep;
+        h->prof = prof;
+        if (rc) { cudaGraph_t junk; cudaStreamEndCapture(b->origin, &junk); if (junk) cudaGraphDestroy(junk); return rc; }
+    }
+    for (int l = 0; l < b->width; ++l) {
+        BCK(cudaEventRecord(b->ev[1 + l], b->lanes[l]));
+        BCK(cudaStreamWaitEvent(b->origin, b->ev[1 + l], 0));
+    }
+    BCK(cudaStreamEndCapture(b->origin, &gr));
+    cudaError_t e = cudaGraphInstantiate(&b->exec, gr, 0);
+    cudaGraphDestroy(gr);
+    BCK(e);
+    BCK(cudaGetLastError());
+    b->exec_steps = nsteps;
+    return FGPE_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1451,6 +1656,7 @@ int fgpe_batch_destroy(fgpe_batch_t* b) {
     if (!b) return FGPE_OK;
     if (b->origin) cudaStreamSynchronize(b->origin);
     drop_graph(b);
+    free_groups(b);
     for (cudaStream_t s : b->lanes) cudaStreamDestroy(s);
     for (cudaEvent_t e : b->ev) cudaEventDestroy(e);
     if (b->origin) cudaStreamDestroy(b->origin);
@@ -1498,7 +1704,13 @@ int fgpe_batch_step(fgpe_batch_t* b, int nsteps) {
             left -= 1;
             continue;
         }
-        if (!b->exec || b->exec_steps != k) { int r = capture(b, k); if (r) return r; }
+        if (!b->exec || b->exec_steps != k) {
+            int r = b->mode == FGPE_BATCH_GROUPED ? capture_grouped(b, k) : capture(b, k);
+            if (r) return r;
+        } else if (b->mode == FGPE_BATCH_GROUPED) {
+            int r = refresh_descs(b);
+            if (r) return r;
+        }
         BCK(cudaGraphLaunch(b->exec, b->origin));
         for (fgpe_t* h : b->inst) h->launches += step_launches(h, k);
         left -= k;
@@ -1524,7 +1736,8 @@ int fgpe_batch_step_timed(fgpe_batch_t* b, int nsteps, double* device_ms) {
     while (err == cudaSuccess && rc == FGPE_OK && left > 0) {
         int k = std::min(left, b->ksteps);
         if (k == 1) k = 2;   // cannot happen: remainder 1 rejected above
-        if (!b->exec || b->exec_steps != k) rc = capture(b, k);
+        if (!b->exec || b->exec_steps != k) rc = b->mode == FGPE_BATCH_GROUPED ? capture_grouped(b, k) : capture(b, k);
+        else if (b->mode == FGPE_BATCH_GROUPED) rc = refresh_descs(b);
         if (rc) break;
         err = cudaGraphLaunch(b->exec, b->origin);
         for (fgpe_t* h : b->inst) h->launches += step_launches(h, k);
@@ -1593,14 +1806,18 @@ int fgpe_batch_autotune(fgpe_batch_t* b, int trial_steps, const char* cache_path
             while (fgets(line, sizeof line, f)) {
                 std::string l(line);
                 if (l.compare(0, sig.size() + 1, sig + " ") != 0) continue;
-                int w = 0, k = 0;
+                int w = 0, k = 0, md = FGPE_BATCH_BRANCHES;
+                double tms = 0;
                 char fam[4096] = {0};
-                if (sscanf(l.c_str() + sig.size() + 1, "%d %d %4095s", &w, &k, fam) == 3) {
+                const int got = sscanf(l.c_str() + sig.size() + 1, "%d %d %4095s %lf %d", &w, &k, fam, &tms, &md);
+                if (got >= 3) {
                     fclose(f);
                     std::string fs(fam);
                     for (size_t ci = 0; ci < classes.size() && ci < fs.size(); ++ci)
                         for (int i = 0; i < n; ++i)
                             if (sizes[i] == classes[ci]) fgpe_set_kernels(b->inst[i], fs[ci] == 'g' ? FGPE_KERNELS_GENERIC : FGPE_KERNELS_AUTO);
+                    const int rm = fgpe_batch_mode(b, got >= 5 ? md : FGPE_BATCH_BRANCHES);
+                    if (rm) return rm;
                     return fgpe_batch_config(b, w, k);
                 }
             }
@@ -1687,8 +1904,8 @@ int fgpe_batch_autotune(fgpe_batch_t* b, int trial_steps, const char* cache_path
             if (sizes[i] == classes[ci]) fgpe_set_kernels(b->inst[i], pick ? FGPE_KERNELS_GENERIC : FGPE_KERNELS_AUTO);
         best_ms = std::min(tms[0], tms[1]);
     }
-    // 2) branch width and steps per graph
-    int bw = std::min(n, 64), bk = 8;
+    // 2) branch width and steps per graph, one branch per instance
+    int bw = std::min(n, 64), bk = 8, bmode = FGPE_BATCH_BRANCHES;
     const int widths[] = {4, 16, 32, 64, 128, 256, 512};
     const int ks[] = {4, 8, 32};
     for (int w : widths) {
@@ -1700,6 +1917,19 @@ int fgpe_batch_autotune(fgpe_batch_t* b, int trial_steps, const char* cache_path
             if (ms < best_ms) { best_ms = ms; bw = w; bk = k; }
         }
     }
+    // 3) grouped launches (instances of one q2D grid shape share each pass)
+    {
+        int r = fgpe_batch_mode(b, FGPE_BATCH_GROUPED);
+        if (r) return finish(r);
+        for (int k : ks) {
+            double ms = 0;
+            r = timed(std::min(n, 64), k, &ms);
+            if (r) return finish(r);
+            if (ms < best_ms) { best_ms = ms; bw = std::min(n, 64); bk = k; bmode = FGPE_BATCH_GROUPED; }
+        }
+        r = fgpe_batch_mode(b, bmode);
+        if (r) return finish(r);
+    }
 #undef ACK
     int r = finish(FGPE_OK);
     if (r) return r;
@@ -1707,7 +1937,18 @@ int fgpe_batch_autotune(fgpe_batch_t* b, int trial_steps, const char* cache_path
     if (r) return r;
     if (cache_path) {
         FILE* f = fopen(cache_path, "a");
-        if (f) { fprintf(f, "%s %d %d %s %.6f\n", sig.c_str(), bw, bk, fam.c_str(), best_ms); fclose(f); }
+        if (f) { fprintf(f, "%s %d %d %s %.6f %d\n", sig.c_str(), bw, bk, fam.c_str(), best_ms, bmode); fclose(f); }
+    }
+    return FGPE_OK;
+}
+
+int fgpe_batch_mode(fgpe_batch_t* b, int mode) {
+    if (!b) return bfail(b, FGPE_E_ARG, "null batch");
+    if (mode != FGPE_BATCH_BRANCHES && mode != FGPE_BATCH_GROUPED) return bfail(b, FGPE_E_ARG, "unknown batch mode");
+    if (mode != b->mode) {
+        drop_graph(b);
+        free_groups(b);
+        b->mode = mode;
     }
     return FGPE_OK;
 }

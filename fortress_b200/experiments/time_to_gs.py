@@ -1,0 +1,324 @@
+"""Time to the 3D spin-1 ground state: learned guess + FP32 against plain FP64.
+
+Target problem (the largest configuration): 3D spin-1 SO-coupled imaginary
+time on 256^3 points, DX=DY=DZ=0.1, DT=1e-3, Rb-87 a0/a2 = 101.8/100.4 a_B,
+NATOMS=1e5, NU=(50,50,50) Hz, GAMMA=(0.5,0.5,0.5).  The quantity measured is
+the wall time until |E - E*| <= 1e-8 |E*| holds for good (energy checked
+every STP = 100 steps, as the reference's loop checks its stop rule,
+cgpe3d.f90:497-508), with E* the FP64 energy after a long run past
+convergence.  Arms, all on one B200 from the same seeded start where a start
+is needed:
+
+  plain      INITIALIZE's 3D spin-1 Gaussian (cgpe3d.f90:783-785) x (1 + 1e-3
+             U[0,1), PCG64 seed 3), FP64 throughout: the reference's method.
+  learned    the 3D Fourier neural operator (fortress_b200.fno3d), trained on
+             ground states the solver computed on a 64^3 grid of the same box
+             over a parameter box around the target, evaluated directly on the
+             256^3 grid (inference time counted); then the FP32-bulk path to
+             its own stop rule (CONV or CONV_EN <= 1e-6), then FP64.
+  learned64  the same guess, FP64 throughout (the network's own gain).
+  coarse     no network: the plain start solved on the 64^3 grid (FP64, to the
+             stop rule at 1e-8), spectrally prolonged to 256^3 (zero padding
+             of the 64^3 spectrum), then FP32 and FP64 as in "learned" (the
+             coarse-to-fine gain without learning).
+
+The target parameter point is held out of the training set (the training
+points are drawn from the box with seed 5 and none coincides with it).
+
+    python -m fortress_b200.experiments.time_to_gs [--train 192] [--epochs 60] [--out DIR]
+
+Prints one JSON object per stage; the last one is the comparison.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import time
+
+import numpy as np
+
+L_BOX = 25.6
+STP = 100
+TOL_REL = 1e-8
+
+
+# ------------------------------------------------------------- parameters
+def target_point():
+    """(gamma, c0, c2/c0, NUZ/NUX) of the 256^3 workload (c0 = TAU(0)/2)."""
+    from fortress_b200.config import RunConfig
+    c = RunConfig(dim=3, spin=1, n=(256, 256, 256), d=(0.1, 0.1, 0.1), dt=1e-3, mass=87.0, a=(101.8, 100.4, 0.0),
+                  natoms=100000, nu=(50.0, 50.0, 50.0), switch_im=1, gamma=(0.5, 0.5, 0.5))
+    t = c.tau()
+    return np.array([0.5, t[0] / 2.0, t[1] / t[0], 1.0])
+
+
+def box_points(count, seed):
+    from fortress_b200.fno3d import BOX3
+    rng = np.random.default_rng(seed)
+    lo = np.array([v[0] for v in BOX3.values()])
+    hi = np.array([v[1] for v in BOX3.values()])
+    return lo + (hi - lo) * rng.uniform(size=(count, 4))
+
+
+def params(point, n, precision="fp64", dt=1e-3):
+    g, c0, r2, az = (float(v) for v in point)
+    d = L_BOX / n
+    return dict(dim=3, spin=1, n=(n, n, n), d=(d, d, d), dt=dt, imag_time=True, tau=(2 * c0, 2 * c0 * r2, 0.0),
+                gamma=(g, g, g), alpha=(1.0, 1.0, az), precision=precision)
+
+
+def gaussian_start(n, seed=3):
+    """INITIALIZE's 3D spin-1 default: the unweighted Gaussian in every
+    component (cgpe3d.f90:783-785), times (1 + 1e-3 u), u ~ U[0,1)."""
+    d = L_BOX / n
+    x = (-1.0 + 2.0 * np.arange(n) / n) * n * d / 2.0
+    g = np.exp(-(x[:, None, None] ** 2 + x[None, :, None] ** 2 + x[None, None, :] ** 2) / 2.0) / np.pi ** 0.75
+    rng = np.random.default_rng(seed)
+    phi = np.empty((n, n, n, 3), np.complex128)
+    for m in range(3):
+        phi[..., m] = g * (1.0 + 1e-3 * rng.uniform(size=g.shape))
+    return phi
+
+
+# ------------------------------------------------------------ training data
+def ground_states(points, n, steps, precision="fp32", chunk=64):
+    """Imaginary-time ground states of every point on the n^3 grid, in
+    batches of `chunk` instances (fortress_b200.batch); returns complex64
+    PHI arrays [count, n, n, n, 3] and the final CONV of each."""
+    import torch
+    from fortress_b200.batch import Batch
+    start = gaussian_start(n)
+    out = np.empty((len(points), n, n, n, 3), np.complex64)
+    conv = np.empty(len(points))
+    for c0 in range(0, len(points), chunk):
+        pts = points[c0:c0 + chunk]
+        b = Batch([params(p, n, precision) for p in pts])
+        for i in range(len(pts)):
+            b[i].set_state(start)
+            b[i].normt()
+        b.step(steps)
+        torch.cuda.synchronize()
+        obs = b.observables(with_conv=True)
+        for i in range(len(pts)):
+            out[c0 + i] = b[i].state()
+            conv[c0 + i] = obs[i]["conv"] / (2.0 * params(pts[i], n)["dt"])
+        b.close()
+    return out, conv
+
+
+def targets(states):
+    """[6][B][Z][Y][X] float32 training targets from PHI arrays."""
+    s = np.transpose(states, (4, 0, 3, 2, 1))           # [m][B][Z][Y][X]
+    t = np.empty((6,) + s.shape[1:], np.float32)
+    t[0::2] = s.real
+    t[1::2] = s.imag
+    return t
+
+
+def train(points, states, n, epochs, batch, lr, seed=0, width=16, modes=8, layers=4, hidden=64):
+    import torch
+    from fortress_b200 import fno3d as F3
+    net = F3.FNO3(n, batch, width=width, modes=modes, layers=layers, hidden=hidden, seed=seed)
+    pn = np.stack([F3.normalise_params(*p) for p in points])
+    tg = targets(states)
+    rng = np.random.default_rng(seed)
+    nb = len(points) // batch
+    hist = []
+    total = epochs * nb
+    it = 0
+    for ep in range(epochs):
+        perm = rng.permutation(len(points))
+        el = 0.0
+        for k in range(nb):
+            idx = perm[k * batch:(k + 1) * batch]
+            a = F3.input_channels(pn[idx], n)
+            t = torch.tensor(np.ascontiguousarray(tg[:, idx].reshape(6, -1)), device="cuda")
+            net.forward(a)
+            net.loss(t)
+            net.backward()
+            net.adam(lr=lr * 0.5 * (1.0 + math.cos(math.pi * it / total)))
+            it += 1
+            el += float(net.loss_dev.item())
+        hist.append(el / nb)
+    torch.cuda.synchronize()
+    assert not net.tc_error()
+    return net, hist
+
+
+# --------------------------------------------------------------- the arms
+class Clock:
+    def __init__(self):
+        import torch
+        torch.cuda.synchronize()
+        self.t0 = time.perf_counter()
+
+    def __call__(self):
+        return time.perf_counter() - self.t0
+
+
+def run_to(prop, clock, trace, label, max_steps, stop_rule=None, dt=1e-3):
+    """STP-step blocks with ENERGY and CONV after each, appending
+    (label, step, wall, E, CONV, CONV_EN) to trace; stops at max_steps or
+    when stop_rule(conv, conv_en) holds."""
+    en_old = prop.observables()[0]
+    done = 0
+    while done < max_steps:
+        prop.step(STP)
+        done += STP
+        en = prop.observables()[0]
+        c = prop.conv() / (STP * 2.0 * dt)
+        ce = abs(en - en_old) / (STP * 2.0 * dt)
+        en_old = en
+        trace.append((label, done, clock(), en, c, ce))
+        if stop_rule is not None and stop_rule(c, ce):
+            break
+    return done
+
+
+def learned_guess_device(net, point, n):
+    """Network output at n^3 as a device complex128 PHI array (x fastest)."""
+    import torch
+    from fortress_b200 import fno3d as F3
+    net.set_inputs_device(F3.normalise_params(*point)[None, :])
+    net.forward()
+    o = net.out.reshape(6, n, n, n)
+    return torch.complex(o[0::2].double(), o[1::2].double()).contiguous()   # [m][z][y][x] = PHI layout
+
+
+def prolong(phi64_dev, n):
+    """Spectral prolongation of a device PHI array [m][z][y][x] from its grid
+    to n^3 (zero padding of the spectrum; same box, so the values scale by
+    nothing once the FFT normalisations cancel)."""
+    import torch
+    m = phi64_dev.shape[-1]
+    spec = torch.fft.fftn(phi64_dev, dim=(1, 2, 3))
+    h = m // 2
+    big = torch.zeros((3, n, n, n), dtype=spec.dtype, device=spec.device)
+    idx = list(range(h)) + list(range(n - h, n))
+    src = list(range(h)) + list(range(m - h, m))
+    ii = torch.tensor(idx, device=spec.device)
+    ss = torch.tensor(src, device=spec.device)
+    big[:, ii[:, None, None], ii[None, :, None], ii[None, None, :]] = \
+        spec[:, ss[:, None, None], ss[None, :, None], ss[None, None, :]]
+    return (torch.fft.ifftn(big, dim=(1, 2, 3)) * (n / m) ** 3).contiguous()
+
+
+def arm(kind, point, n, clock_state=None, net=None, max_steps=60000, fp32_tol=1e-6):
+    """One arm on the n^3 grid; returns its trace."""
+    import fortress_b200 as F
+    import torch
+    trace = []
+    clock = Clock()
+    p64 = F.Propagator(**params(point, n, "fp64"))
+    if kind == "plain":
+        p64.set_state(gaussian_start(n))
+        p64.normt()
+        trace.append((kind, 0, clock(), p64.observables()[0], float("nan"), float("nan")))
+        run_to(p64, clock, trace, "fp64", max_steps)
+        p64.close()
+        return trace
+    if kind in ("learned", "learned64"):
+        guess = learned_guess_device(net, point, n)
+    else:   # coarse: 64^3 FP64 solve to the stop rule at 1e-8, then prolong
+        pc = F.Propagator(**params(point, 64, "fp64"))
+        pc.set_state(gaussian_start(64))
+        pc.normt()
+        run_to(pc, clock, trace, "coarse64", 200000, stop_rule=lambda c, ce: c <= 1e-8 or ce <= 1e-8)
+        buf = torch.empty((3, 64, 64, 64), dtype=torch.complex128, device="cuda")
+        pc.get_state_device(buf.data_ptr())
+        pc.close()
+        guess = prolong(buf, n)
+    torch.cuda.synchronize()
+    trace.append(("guess", 0, clock(), float("nan"), float("nan"), float("nan")))
+    if kind != "learned64":
+        p32 = F.Propagator(**params(point, n, "fp32"))
+        p32.set_state_device(guess.data_ptr())
+        p32.normt()
+        run_to(p32, clock, trace, "fp32", max_steps, stop_rule=lambda c, ce: c <= fp32_tol or ce <= fp32_tol)
+        buf = torch.empty_like(guess)
+        p32.get_state_device(buf.data_ptr())
+        p32.close()
+        guess = buf
+    p64.set_state_device(guess.data_ptr())
+    p64.normt()
+    del guess
+    trace.append(("switch", 0, clock(), p64.observables()[0], float("nan"), float("nan")))
+    run_to(p64, clock, trace, "fp64", max_steps)
+    p64.close()
+    return trace
+
+
+def time_to(trace, e_star, tol=TOL_REL):
+    """(steps per stage, wall) at the first FP64 energy check after which
+    every later check satisfies |E - E*| <= tol |E*|; None if never."""
+    seen, out = {}, None
+    for lab, st, wall, en, c, ce in trace:
+        if st == 0:
+            continue
+        seen[lab] = st
+        if lab == "fp64":
+            ok = abs(en - e_star) <= tol * abs(e_star)
+            if ok and out is None:
+                out = (dict(seen), wall)
+            elif not ok:
+                out = None
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--train", type=int, default=192)
+    ap.add_argument("--n-train", type=int, default=64)
+    ap.add_argument("--gen-steps", type=int, default=8000)
+    ap.add_argument("--epochs", type=int, default=60)
+    ap.add_argument("--batch", type=int, default=4)
+    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--max-steps", type=int, default=40000)
+    ap.add_argument("--arms", default="plain,learned,learned64,coarse")
+    ap.add_argument("--out", default=None)
+    args = ap.parse_args()
+    out = args.out or os.environ.get("FGPE_BENCH_OUT") or "."
+    os.makedirs(out, exist_ok=True)
+    import torch
+    pts = box_points(args.train, seed=5)
+    tp = target_point()
+    t0 = time.perf_counter()
+    states, conv = ground_states(pts, args.n_train, args.gen_steps)
+    print(json.dumps({"stage": "data", "count": len(pts), "grid": args.n_train, "steps": args.gen_steps,
+                      "seconds": time.perf_counter() - t0, "conv_median": float(np.median(conv)),
+                      "conv_max": float(conv.max())}), flush=True)
+    t0 = time.perf_counter()
+    net, hist = train(pts, states, args.n_train, args.epochs, args.batch, args.lr)
+    print(json.dumps({"stage": "train", "epochs": args.epochs, "seconds": time.perf_counter() - t0,
+                      "loss_first": hist[0], "loss_last": hist[-1]}), flush=True)
+    params_np = net.params_numpy()
+    np.savez(os.path.join(out, "fno3d_params.npz"), **params_np)
+    del net, states
+    torch.cuda.empty_cache()
+    from fortress_b200 import fno3d as F3
+    infer = F3.FNO3(args.n, 1, params=params_np, train=False)
+    traces = {}
+    for kind in args.arms.split(","):
+        traces[kind] = arm(kind, tp, args.n, net=infer, max_steps=args.max_steps)
+        last = traces[kind][-1]
+        print(json.dumps({"stage": "arm", "arm": kind, "wall": last[2], "E_final": last[3],
+                          "fp64_steps": last[1]}), flush=True)
+    e_star = min(tr[-1][3] for tr in traces.values())
+    res = {"stage": "result", "E_star": e_star, "tol_rel": TOL_REL, "grid": args.n, "arms": {}}
+    for kind, tr in traces.items():
+        t = time_to(tr, e_star)
+        res["arms"][kind] = {"time_to_tol_s": t[1] if t else None, "steps": t[0] if t else None,
+                             "E_final": tr[-1][3], "E_final_minus_Estar_rel": (tr[-1][3] - e_star) / abs(e_star)}
+    if res["arms"].get("plain", {}).get("time_to_tol_s") and res["arms"].get("learned", {}).get("time_to_tol_s"):
+        res["speedup_learned_fp32_vs_plain_fp64"] = res["arms"]["plain"]["time_to_tol_s"] / \
+            res["arms"]["learned"]["time_to_tol_s"]
+    with open(os.path.join(out, "time_to_gs.json"), "w") as f:
+        json.dump({"result": res, "traces": traces}, f)
+    print(json.dumps(res), flush=True)
+
+
+if __name__ == "__main__":
+    main()

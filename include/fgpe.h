@@ -190,6 +190,17 @@ int fgpe_batch_step_timed(fgpe_batch_t *b, int nsteps, double *device_ms);
  * of the last step, or -1), MU[M_i], RMS[M_i], NORM[M_i]. */
 int fgpe_batch_observables(fgpe_batch_t *b, double *out, int with_conv);
 
+/* Launch organisation of a batch.  FGPE_BATCH_BRANCHES (the default): every
+ * instance's passes are launches of their own, in parallel graph branches.
+ * FGPE_BATCH_GROUPED: instances that share a q2D grid shape, spin and
+ * precision (both axes of a size-specialised length: 128, 192, 256, 384,
+ * 512) advance together, one column-pass and one row-pass launch per step
+ * for the whole group, each launch walking the tiles of all its instances;
+ * the other instances keep their own branches.  The results are those of
+ * the single-instance passes up to the NORMC summation order. */
+enum { FGPE_BATCH_BRANCHES = 0, FGPE_BATCH_GROUPED = 1 };
+int fgpe_batch_mode(fgpe_batch_t *b, int mode);
+
 /* Autotuner: times kernel family per grid-size class, branch width and
  * steps per graph on the batch itself (states saved and restored) and keeps
  * the fastest; cache_path (may be NULL) remembers the choice per batch

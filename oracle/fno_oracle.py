@@ -129,3 +129,116 @@ def loss_and_grad(p, a, target, modes=16, layers=4):
     g["bP"] = dh.sum(axis=(0, 2, 3))
     g["P"] = np.einsum("boij,bcij->oc", dh, st["a"])
     return loss, g
+
+
+# ------------------------------------------------------------------- 3D form
+# The same network on an N x N x N grid (fortress_b200/fno3d.py):
+#   K h: H_c = sum_{xyz} h_c(x,y,z) e^{-2 pi i (kx x + ky y + kz z)/N} over
+#        kx in {0..M-1} and ky, kz in {0..M-1, N-M..N-1};
+#        G_o = sum_c R_oc * H_c;  K_o = Re(sum_k w_kx G_o e^{+2 pi i k.r/N}) / N^3
+#        with w = 1 for kx = 0 and 2 otherwise.
+# Arrays are [B, C, Z, Y, X] (x fastest).
+def dft_mats3(n, modes):
+    kf = np.concatenate([np.arange(modes), np.arange(n - modes, n)])
+    kh = np.arange(modes)
+    i = np.arange(n)
+    Ef = np.exp(-2j * np.pi * np.outer(i, kf) / n)     # [n, 2M]  (y and z)
+    Eh = np.exp(-2j * np.pi * np.outer(i, kh) / n)     # [n, M]   (x)
+    w = np.where(kh == 0, 1.0, 2.0)
+    return Ef, Eh, w
+
+
+def init_params3(width=16, modes=8, layers=4, cin=7, hidden=64, cout=6, seed=0):
+    rng = np.random.default_rng(seed)
+    p = {"P": rng.standard_normal((width, cin)) / np.sqrt(cin), "bP": np.zeros(width)}
+    for l in range(layers):
+        p[f"W{l}"] = rng.standard_normal((width, width)) / np.sqrt(width)
+        p[f"b{l}"] = np.zeros(width)
+        sc = 1.0 / (width * width)
+        p[f"Rr{l}"] = sc * rng.uniform(size=(width, width, 2 * modes, 2 * modes, modes))
+        p[f"Ri{l}"] = sc * rng.uniform(size=(width, width, 2 * modes, 2 * modes, modes))
+    p["Q1"] = rng.standard_normal((hidden, width)) / np.sqrt(width)
+    p["c1"] = np.zeros(hidden)
+    p["Q2"] = rng.standard_normal((cout, hidden)) / np.sqrt(hidden)
+    p["c2"] = np.zeros(cout)
+    return p
+
+
+def spectral3(h, Rr, Ri, Ef, Eh, w):
+    """h [B, C, Z, Y, X] -> K h and the mode coefficients H [B, C, kz, ky, kx]."""
+    n = h.shape[-1]
+    H = np.einsum("zc,yb,xa,kizyx->kicba", Ef, Ef, Eh, h, optimize=True)
+    G = np.einsum("oicba,kicba->kocba", Rr + 1j * Ri, H, optimize=True)
+    Gt = G * w[None, None, None, None, :]
+    K = np.einsum("zc,yb,xa,kocba->kozyx", np.conj(Ef), np.conj(Ef), np.conj(Eh), Gt, optimize=True).real
+    return K / n ** 3, H
+
+
+def spectral3_bwd(dK, H, Rr, Ri, Ef, Eh, w):
+    n = dK.shape[-1]
+    R = Rr + 1j * Ri
+    # K = Re(A(Gt))/n^3 with A linear: grad wrt Gt = conj(A^T dK)/n^3
+    gGt = np.conj(np.einsum("zc,yb,xa,kozyx->kocba", np.conj(Ef), np.conj(Ef), np.conj(Eh), dK,
+                            optimize=True)) / n ** 3
+    gG = gGt * w[None, None, None, None, :]
+    gR = np.einsum("kocba,kicba->oicba", gG, np.conj(H), optimize=True)
+    gH = np.einsum("kocba,oicba->kicba", gG, np.conj(R), optimize=True)
+    dh = np.einsum("zc,yb,xa,kicba->kizyx", Ef, Ef, Eh, np.conj(gH), optimize=True).real
+    return dh, gR.real, gR.imag
+
+
+def _pw(Wm, x):
+    return np.einsum("oc,bczyx->bozyx", Wm, x, optimize=True)
+
+
+def _bias(b):
+    return b[None, :, None, None, None]
+
+
+def forward3(p, a, modes=8, layers=4, cache=False):
+    """a [B, cin, N, N, N] -> out [B, 6, N, N, N]."""
+    n = a.shape[-1]
+    Ef, Eh, w = dft_mats3(n, modes)
+    h = _pw(p["P"], a) + _bias(p["bP"])
+    st = {"a": a, "h": [h], "z": [], "H": []}
+    for l in range(layers):
+        K, H = spectral3(h, p[f"Rr{l}"], p[f"Ri{l}"], Ef, Eh, w)
+        z = _pw(p[f"W{l}"], h) + _bias(p[f"b{l}"]) + K
+        h = gelu(z) if l < layers - 1 else z
+        st["z"].append(z); st["H"].append(H); st["h"].append(h)
+    u = _pw(p["Q1"], h) + _bias(p["c1"])
+    q = gelu(u)
+    out = _pw(p["Q2"], q) + _bias(p["c2"])
+    st.update(u=u, q=q)
+    return (out, st) if cache else out
+
+
+def loss_and_grad3(p, a, target, modes=8, layers=4):
+    out, st = forward3(p, a, modes, layers, cache=True)
+    n = a.shape[-1]
+    Ef, Eh, w = dft_mats3(n, modes)
+    diff = out - target
+    loss = float(np.mean(diff ** 2))
+    g = {}
+    red = (0, 2, 3, 4)
+    dout = 2.0 * diff / diff.size
+    g["c2"] = dout.sum(axis=red)
+    g["Q2"] = np.einsum("bozyx,bczyx->oc", dout, st["q"], optimize=True)
+    dq = np.einsum("oc,bozyx->bczyx", p["Q2"], dout, optimize=True)
+    du = dq * gelu_grad(st["u"])
+    g["c1"] = du.sum(axis=red)
+    g["Q1"] = np.einsum("bozyx,bczyx->oc", du, st["h"][-1], optimize=True)
+    dh = np.einsum("oc,bozyx->bczyx", p["Q1"], du, optimize=True)
+    for l in reversed(range(layers)):
+        z = st["z"][l]
+        dz = dh * gelu_grad(z) if l < layers - 1 else dh
+        hin = st["h"][l]
+        g[f"b{l}"] = dz.sum(axis=red)
+        g[f"W{l}"] = np.einsum("bozyx,bczyx->oc", dz, hin, optimize=True)
+        dh_lin = np.einsum("oc,bozyx->bczyx", p[f"W{l}"], dz, optimize=True)
+        dh_sp, gRr, gRi = spectral3_bwd(dz, st["H"][l], p[f"Rr{l}"], p[f"Ri{l}"], Ef, Eh, w)
+        g[f"Rr{l}"], g[f"Ri{l}"] = gRr, gRi
+        dh = dh_lin + dh_sp
+    g["bP"] = dh.sum(axis=red)
+    g["P"] = np.einsum("bozyx,bczyx->oc", dh, st["a"], optimize=True)
+    return loss, g

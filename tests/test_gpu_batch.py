@@ -96,3 +96,64 @@ def test_timed_batch_step(F):
         assert np.array_equal(a[i].state(), b[i].state())
     with pytest.raises(F.FgpeError):
         b.step_timed(9)            # 4 + 4 + 1
+
+
+def _grouped_instances():
+    """Two instances per group (128^2 spin-1 FP64 imaginary, 192x128 spin-2
+    FP32 real time, 512^2 and 384x256 spin-1 FP64) plus one instance of a
+    size the grouped kernels do not cover (on its own branch)."""
+    rng = np.random.default_rng(9)
+    out = []
+    for n, spin, imag, prec in [((128, 128), 1, 1, "fp64"), ((128, 128), 1, 1, "fp64"),
+                                ((192, 128), 2, 0, "fp32"), ((192, 128), 2, 0, "fp32"),
+                                ((512, 512), 1, 1, "fp64"), ((384, 256), 1, 0, "fp64"),
+                                ((384, 256), 1, 0, "fp64"), ((96, 80), 1, 1, "fp64")]:
+        p = case_params((2, spin, imag, n))
+        p["gamma"] = tuple(rng.uniform(0, 2, 2))
+        if spin == 1:
+            p["tau"] = (float(rng.uniform(200, 4000)), float(rng.uniform(-0.05, 0.05) * 2000), 0.0)
+        p["alpha"] = (1.0, float(rng.uniform(1, 2)), 1.0)
+        p["d"] = (25.6 / n[0], 25.6 / n[1])
+        p["precision"] = prec
+        out.append(p)
+    return out
+
+
+def _guess_ms(p, seed):
+    ms = 2 * p["spin"] + 1
+    g = _guess(p, seed)[..., :1]
+    rng = np.random.default_rng(seed + 1)
+    return np.concatenate([g * (1 + 0.05 * rng.standard_normal(g.shape)) for _ in range(ms)], axis=-1)
+
+
+def test_grouped_batch_matches_individual(F):
+    """Grouped launches (one pass launch per group of equal grid shapes)
+    against each instance stepped alone: the same per-tile arithmetic, so
+    the states agree to the rounding of the NORMC summation order (bitwise in
+    real time), and NORMC, the observables and CONV agree likewise."""
+    from fortress_b200.batch import Batch
+    insts = _grouped_instances()
+    b = Batch(insts)
+    b.mode(grouped=True)
+    singles = [F.Propagator(**p) for p in insts]
+    for i, p in enumerate(insts):
+        phi = _guess_ms(p, 20 + i)
+        for x in (b[i], singles[i]):
+            x.set_state(phi)
+            if p["imag_time"]:
+                x.normt()
+    b.config(width=4, steps_per_graph=5)
+    b.step(12)                    # graphs of 5, 5 and 2 steps
+    for s in singles:
+        s.step(12)
+    obs = b.observables()
+    for i, p in enumerate(insts):
+        tol = 1e-13 if p["precision"] == "fp64" else 2e-6
+        sa, sb = b[i].state(), singles[i].state()
+        if not p["imag_time"]:
+            assert np.array_equal(sa, sb), i
+        assert np.abs(sa - sb).max() <= tol * np.abs(sb).max(), i
+        assert np.allclose(b[i].normc(), singles[i].normc(), rtol=1e-12, atol=0), i
+        en, mu, mz, rms = singles[i].observables()
+        assert abs(obs[i]["en"] - en) <= 1e-12 * abs(en) and np.allclose(obs[i]["rms"], rms, rtol=1e-12), i
+        assert abs(obs[i]["conv"] - singles[i].conv()) <= 1e-10 * max(singles[i].conv(), 1e-12), i
