@@ -381,14 +381,14 @@ def kernel_pass(prop, flush, steps):
 KCLASS = ["row_x", "col_y", "col_z", "oned"]
 
 
-def device_rate(F, w, phi, precision, steps, warmup, stream, flush, world, dist):
+def device_rate(F, w, phi, precision, steps, warmup, stream, flush, world, dist, kernels="auto"):
     """value of one precision: K split steps on the device between CUDA
     events on the launching stream (max over ranks), plus the per-kernel
     pass.  Returns a dict and the propagator."""
     import numpy as np
     import torch
     cfg = run_config(w)
-    prop = F.Propagator(**cfg.params(precision))
+    prop = F.Propagator(**cfg.params(precision), kernels=kernels)
     prop.set_stream(stream.cuda_stream)
     prop.set_state(phi)
     if cfg.switch_im:
@@ -512,7 +512,8 @@ def ours(args, w, rank, world, local_rank):
 
     clocks = ClockSampler(local_rank)
     clocks.start()
-    main, prop = device_rate(F, w, phi, args.precision, args.steps, args.warmup, stream, flush, world, dist)
+    main, prop = device_rate(F, w, phi, args.precision, args.steps, args.warmup, stream, flush, world, dist,
+                             args.kernels)
     clk = clocks.stop()
     rl, kernels = roofline(w, args.precision, main["kms"], main["kn"], peak, peak_kind, fp64_peak)
 
@@ -533,7 +534,7 @@ def ours(args, w, rank, world, local_rank):
         "e2e": e2e, "gpu_launches": main["launches"], "roofline": rl, "kernels": kernels, "clocks": clk,
     }
     if args.precision == "fp64" and not args.no_fp32:
-        f32, p32 = device_rate(F, w, phi, "fp32", args.steps, args.warmup, stream, flush, world, dist)
+        f32, p32 = device_rate(F, w, phi, "fp32", args.steps, args.warmup, stream, flush, world, dist, args.kernels)
         p32.close()
         rl32, k32 = roofline(w, "fp32", f32["kms"], f32["kn"], peak, peak_kind, fp64_peak)
         result["fp32"] = {"value": f32["value"], "ms_per_step": f32["ms_per_step"], "dtype": "c64",
@@ -692,6 +693,50 @@ def sweep(args):
     return 0
 
 
+def time_to_ground_state(args):
+    """Time to the 256^3 spin-1 ground state: wall time until
+    |E - E*| <= 1e-8 |E*| holds for good (energy every 100 steps), E* the
+    lowest final FP64 energy of the arms.  Arms (fortress_b200.experiments.
+    time_to_gs): plain FP64 from INITIALIZE's seeded Gaussian (the
+    reference's method); coarse (64^3 FP64 solve, spectral prolongation,
+    FP32 to its stop rule, then FP64); learned (the trained 3D network's
+    guess, FP32, then FP64) when --fno3d names a saved parameter file."""
+    import numpy as np
+    import torch
+    from fortress_b200.experiments import time_to_gs as T
+    tp = T.target_point()
+    arms = ["plain", "coarse"]
+    infer = None
+    if args.fno3d:
+        from fortress_b200 import fno3d as F3
+        pz = dict(np.load(args.fno3d))
+        W = pz["P"].shape[0]
+        M = pz["Rr0"].shape[-1]
+        layers = sum(1 for k in pz if k.startswith("Rr"))
+        infer = F3.FNO3(256, 1, params=pz, width=W, modes=M, layers=layers, hidden=pz["Q1"].shape[0], train=False)
+        arms.append("learned")
+    clocks = ClockSampler(0)
+    clocks.start()
+    traces = {k: T.arm(k, tp, 256, net=infer, max_steps=args.tts_max_steps) for k in arms}
+    clk = clocks.stop()
+    e_star = min(tr[-1][3] for tr in traces.values())
+    res = {}
+    for k, tr in traces.items():
+        t = T.time_to(tr, e_star)
+        res[k] = {"time_s": t[1] if t else None, "steps": t[0] if t else None,
+                  "E_final_rel_to_Estar": (tr[-1][3] - e_star) / abs(e_star)}
+    best = min((k for k in arms if k != "plain" and res[k]["time_s"]), key=lambda k: res[k]["time_s"], default=None)
+    plain = res["plain"]["time_s"]
+    out = {"metric": "time to |E-E*| <= 1e-8 |E*| (256^3 spin-1 SO ground state)",
+           "value": res[best]["time_s"] if best else None, "unit": "s", "n_gpus": 1, "higher_is_better": False,
+           "scaling": "weak", "vs_baseline": None, "dtype": "c64 then c128", "data": data_string(D3),
+           "config": {"workload": "tts-3d-spin1-SO-256^3", "arm": best, "stp": T.STP, "tol_rel": T.TOL_REL},
+           "E_star": e_star, "arms": res, "plain_fp64_s": plain,
+           "speedup_vs_plain_fp64": (plain / res[best]["time_s"]) if (best and plain) else None, "clocks": clk}
+    print(json.dumps(out))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -701,11 +746,14 @@ def main():
     ap.add_argument("--precision", default=None, choices=["fp64", "fp32"],
                     help="arithmetic of the headline value (default fp64; the fp32 figure is added beside it)")
     ap.add_argument("--no-fp32", action="store_true", help="skip the FP32-bulk figure")
+    ap.add_argument("--kernels", default="auto", choices=["auto", "generic", "warp-row"],
+                    help="kernel family of the timed propagators (fgpe_params.kernels)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="3d", choices=["3d", "q2d", "sweep", "golden1d", "fno", "tour"],
+    ap.add_argument("--workload", default="3d", choices=["3d", "q2d", "sweep", "golden1d", "tts", "fno", "tour"],
                     help="3d: 256^3 spin-1 imaginary time (headline); q2d: 512^2 spin-2 real-time quench; "
                          "sweep: 512 ragged q2D spin-1 instances in one batched graph launch; "
                          "golden1d: the reference's published run (1D spin-2, 2048 points, to convergence); "
+                         "tts: time to the 256^3 spin-1 ground state (plain FP64 against coarse/learned + FP32); "
                          "fno: with --capture only, learned-guess training steps; "
                          "tour: with --capture only, every kernel family once")
     ap.add_argument("--capture", action="store_true",
@@ -713,6 +761,8 @@ def main():
                          "no other work) for profiler captures")
     ap.add_argument("--grid", type=int, default=0, help="with --capture --workload 3d: points per axis (192)")
     ap.add_argument("--observables", action="store_true", help="with --capture: also run ENERGY/RAD (k_obs)")
+    ap.add_argument("--fno3d", default=None, help="with --workload tts: saved 3D network parameters (.npz)")
+    ap.add_argument("--tts-max-steps", type=int, default=40000, help="with --workload tts: steps per FP64 stage")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     args.precision_set = args.precision is not None
@@ -736,6 +786,8 @@ def main():
         return 0
     if args.workload == "golden1d":
         return golden1d(args)
+    if args.workload == "tts":
+        return time_to_ground_state(args)
     return sweep(args)
 
 

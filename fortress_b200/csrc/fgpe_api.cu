@@ -74,6 +74,9 @@ struct fgpe_s {
     bool has_fast_row = false, has_fast_col[3] = {false, false, false};
     int fast_row_grid = 0, fast_col_grid[3] = {0, 0, 0};
     bool col_wide[3] = {false, false, false};   // column pass uses the wide tiles
+    // row pass with one warp per x row (k_row_warp), where a row fits 16 KB
+    bool has_warp_row = false, warp_row = false;
+    int warp_row_grid = 0;
     bool psi_valid = false, S_valid = false, prev_valid = false, norms_valid = false, has_state = false;
     long long launches = 0;
     std::string msg;
@@ -245,6 +248,26 @@ template <typename T, int MS, int N> int setup_fast_col(fgpe_t* h, int n_other, 
     return grid_for(k_col_fast<T, MS, N, col_tx<T>(), col_th<T, MS, N>()>, col_th<T, MS, N>(), col_smem<T, MS, N>(),
                     (h->p.nx / col_tx<T>()) * n_other);
 }
+// Warp-row kernel: rows of MS lines up to 16 KB (FP64 spin-1 to 256 points,
+// spin-2 to 128; FP32 spin-1 to 512, spin-2 to 256); warps per block so that
+// two blocks of NBUF rows per warp fit the shared memory.
+template <typename T, int MS, int N> constexpr size_t wrow_tile() { return (size_t)MS * cpad(N) * sizeof(cx<T>); }
+template <typename T, int MS, int N> constexpr bool wrow_ok() { return wrow_tile<T, MS, N>() <= 16 * 1024; }
+template <typename T, int MS, int N> constexpr int wrow_wpb() {
+    const int w = (int)((110 * 1024) / (wrow_tile<T, MS, N>() * FGPE_WROW_NBUF));
+    return w < 1 ? 1 : (w > 8 ? 8 : w);
+}
+template <typename T, int MS, int N> int setup_warp_row(fgpe_t* h) {
+    if constexpr (!wrow_ok<T, MS, N>()) {
+        return 0;
+    } else {
+        constexpr int W = wrow_wpb<T, MS, N>();
+        const int rows = h->p.ny * h->p.nz;
+        return grid_for(k_row_warp<T, MS, N, W, FGPE_WROW_NBUF>, W * 32,
+                        (size_t)W * FGPE_WROW_NBUF * wrow_tile<T, MS, N>(), (rows + W - 1) / W);
+    }
+}
+
 // The size-specialised kernels go out as programmatic dependent launches
 // (outside stream capture): the next pass is launched while the previous one
 // drains and waits on griddepcontrol.wait before it touches the state.  Their
@@ -273,6 +296,13 @@ void launch_pdl(fgpe_t* h, K kern, int grid, int threads, size_t smem, const A& 
 template <typename T, int MS, int N> void run_fast_row(fgpe_t* h, const RowArgs& a) {
     launch_pdl(h, k_row_fast<T, MS, N, row_r(N), row_th<T, MS, N>()>, h->fast_row_grid, row_th<T, MS, N>(),
                row_smem<T, MS, N>(), a);
+}
+template <typename T, int MS, int N> void run_warp_row(fgpe_t* h, const RowArgs& a) {
+    if constexpr (wrow_ok<T, MS, N>()) {
+        constexpr int W = wrow_wpb<T, MS, N>();
+        launch_pdl(h, k_row_warp<T, MS, N, W, FGPE_WROW_NBUF>, h->warp_row_grid, W * 32,
+                   (size_t)W * FGPE_WROW_NBUF * wrow_tile<T, MS, N>(), a);
+    }
 }
 template <typename T, int MS, int N> void run_fast_col(fgpe_t* h, int axis, const ColArgs& a) {
     if constexpr (wide_ok<T, MS, N>()) {
@@ -326,6 +356,13 @@ void launch_row(fgpe_t* h, int mode, void* snap) {
     a.S = h->S; a.psi = h->psi; a.snap = snap; a.part = h->part; a.counter = h->counters;
     a.info = h->info; a.rows = h->row.tile; a.mode = mode;
     ProfScope ps(h, 0);
+    if (h->warp_row && mode == ROW_FULL) {
+#define RUNW(NN) run_warp_row<T, MS, NN>(h, a)
+        FAST_SWITCH(h->p.nx, RUNW)
+#undef RUNW
+        h->launches++;
+        return;
+    }
     if (h->fast_row) {
 #define RUNR(NN) run_fast_row<T, MS, NN>(h, a)
         FAST_SWITCH(h->p.nx, RUNR)
@@ -836,6 +873,16 @@ int fgpe_create(const fgpe_params* pin, fgpe_t** out) {
         FAST_SWITCH(p.nx, SETR)
 #undef SETR
         if (g > 0) { h->fast_row = h->has_fast_row = true; h->fast_row_grid = g; }
+        int gw = 0;
+#define SETW(NN) gw = h->fp32 ? (ms == 3 ? setup_warp_row<float, 3, NN>(h) : setup_warp_row<float, 5, NN>(h)) \
+                              : (ms == 3 ? setup_warp_row<double, 3, NN>(h) : setup_warp_row<double, 5, NN>(h))
+        FAST_SWITCH(p.nx, SETW)
+#undef SETW
+        if (gw > 0) {
+            h->has_warp_row = true;
+            h->warp_row_grid = gw;
+            h->warp_row = p.kernels == FGPE_KERNELS_WARP_ROW;
+        }
     }
     for (int a = 1; a < p.dim; ++a) {
         if (!allow_fast_col || !fast_size(ns[a])) continue;
@@ -852,7 +899,8 @@ int fgpe_create(const fgpe_params* pin, fgpe_t** out) {
     h->obsl.grid = dim3((unsigned)((h->npts + 255) / 256));
     const size_t nq = 3 * ms + 3;
     const size_t npart = std::max<size_t>(std::max<size_t>((size_t)h->obsl.grid.x * nq,
-                                                           (size_t)std::max<int>(h->row.grid.x, h->fast_row_grid) * ms),
+                                                           (size_t)std::max<int>(std::max<int>(h->row.grid.x, h->fast_row_grid),
+                                                                                 h->warp_row_grid) * ms),
                                           (size_t)h->c1d.grid.x * ms) + 64;
     CK(cudaMalloc(&h->part, npart * sizeof(double)));
     CK(cudaMalloc(&h->info, 4 * INFO_LEN * sizeof(double)));
@@ -1243,6 +1291,7 @@ int fgpe_set_kernels(fgpe_t* h, int kernels) {
     if (h->bulk) { CK(cudaStreamSynchronize(h->st)); cudaGraphExecDestroy(h->bulk); h->bulk = nullptr; }
     const bool fast = kernels != FGPE_KERNELS_GENERIC;
     h->fast_row = fast && h->has_fast_row && kernels != FGPE_KERNELS_FAST_COL_ONLY;
+    h->warp_row = h->has_warp_row && kernels == FGPE_KERNELS_WARP_ROW;
     for (int a = 0; a < 3; ++a) h->fast_col[a] = fast && h->has_fast_col[a] && kernels != FGPE_KERNELS_FAST_ROW_ONLY;
     return FGPE_OK;
 }

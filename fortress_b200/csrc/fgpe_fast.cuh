@@ -61,7 +61,9 @@ template <int N, int TX> struct ColTile {
 // assignment) and the task groups are whole warps, the pass ends on the named
 // barrier of its group (ids 1..15) instead of the block barrier.  NEXT_R is
 // the radix of the next pass of the same transform, 0 after the last.
-template <typename T, bool INV, int N, int NL, int TH, int P, class Map, int NEXT_R = 0>
+// WARP = 1: the lines belong to one warp (TH = 32, tasks by lane) and every
+// pass ends on __syncwarp.
+template <typename T, bool INV, int N, int NL, int TH, int P, class Map, int NEXT_R = 0, int WARP = 0>
 __device__ __forceinline__ void ct_pass(cx<T>* s, const cx<T>* __restrict__ tw) {
     constexpr CPlan pl = cplan(N);
     constexpr int R = pl.r[P];
@@ -69,9 +71,11 @@ __device__ __forceinline__ void ct_pass(cx<T>* s, const cx<T>* __restrict__ tw) 
     constexpr int SI = BP / R, NB = N / R, TOT = NL * NB, ITER = (TOT + TH - 1) / TH, TSTEP = N / BP;
     constexpr int GT = Map::GROUP(NB);
     constexpr bool GROUPED = NEXT_R == R && TOT == TH && GT % 32 == 0 && TOT % GT == 0 && TOT / GT <= 15;
+    static_assert(!WARP || TH == 32, "warp-scope passes run on 32 lanes");
+    const int tid = WARP ? (int)(threadIdx.x & 31) : (int)threadIdx.x;
 #pragma unroll
     for (int it = 0; it < ITER; ++it) {
-        const int b = threadIdx.x + it * TH;
+        const int b = tid + it * TH;
         if ((TOT % TH) == 0 || b < TOT) {
             int l, q; Map::split(b, NB, l, q);
             const int blk = q / SI, n2 = q - blk * SI;
@@ -100,7 +104,9 @@ __device__ __forceinline__ void ct_pass(cx<T>* s, const cx<T>* __restrict__ tw) 
             for (int r = 0; r < R; ++r) s[Map::at(l, e0 + r * SI)] = v[r];
         }
     }
-    if constexpr (GROUPED) {
+    if constexpr (WARP) {
+        __syncwarp();
+    } else if constexpr (GROUPED) {
         const int g = (int)threadIdx.x / GT;
         asm volatile("bar.sync %0, %1;\n" ::"r"(1 + g), "r"(GT) : "memory");
     } else {
@@ -108,14 +114,14 @@ __device__ __forceinline__ void ct_pass(cx<T>* s, const cx<T>* __restrict__ tw) 
     }
 }
 
-template <typename T, bool INV, int N, int NL, int TH, class Map, int P = 0>
+template <typename T, bool INV, int N, int NL, int TH, class Map, int WARP = 0, int P = 0>
 __device__ __forceinline__ void ct_fft(cx<T>* s, const cx<T>* __restrict__ tw) {
     constexpr CPlan pl = cplan(N);
     if constexpr (P < pl.nf) {
         constexpr int PP = INV ? pl.nf - 1 - P : P;
         constexpr int NEXT_R = P + 1 < pl.nf ? pl.r[INV ? PP - 1 : PP + 1] : 0;
-        ct_pass<T, INV, N, NL, TH, PP, Map, NEXT_R>(s, tw);
-        ct_fft<T, INV, N, NL, TH, Map, P + 1>(s, tw);
+        ct_pass<T, INV, N, NL, TH, PP, Map, NEXT_R, WARP>(s, tw);
+        ct_fft<T, INV, N, NL, TH, Map, WARP, P + 1>(s, tw);
     }
 }
 
@@ -288,6 +294,98 @@ __global__ void __launch_bounds__(TH, row_minb(TH)) k_row_fast(StepConst c, RowA
     cp_wait<0>();
     asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
     if (a.mode != ROW_FULL) return;
+    block_sum<MS>(acc, red, bsum);
+    if (threadIdx.x < MS) a.part[(size_t)blockIdx.x * MS + threadIdx.x] = bsum[threadIdx.x];
+    finish_norms<MS>(c, a.part, a.counter, a.info, red);
+}
+
+// ------------------------------------------------------- warp-row kernel
+// The row pass (ROW_FULL) with one warp per x row: the MS component lines of
+// one (y, z) position sit in the warp's private shared memory, so the inverse
+// transform, SE, SP, the NORMC partials and the forward transform need only
+// __syncwarp; the block meets once at the end, for its NORMC partial and the
+// last-block reduction.  Rows are dealt to the warps of the grid in turn;
+// with NBUF = 2 a warp prefetches its next row with cp.async while it works
+// on the current one.  Per element the arithmetic is that of k_row_fast.
+#ifndef FGPE_WROW_NBUF
+#define FGPE_WROW_NBUF 1
+#endif
+template <typename T, int MS, int N, int WPB, int NBUF>
+__global__ void __launch_bounds__(WPB * 32, 2) k_row_warp(StepConst c, RowArgs a) {
+    asm volatile("griddepcontrol.wait;\n" ::: "memory");
+    using RT = RowTile<N, MS>;
+    constexpr int LP = RT::LP;
+    constexpr int TILE = MS * LP;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const int warp = (int)(threadIdx.x >> 5), lane = (int)(threadIdx.x & 31);
+    cx<T>* mine = (cx<T>*)smraw + (size_t)warp * NBUF * TILE;
+    __shared__ double red[32 * (MS + 1)];
+    __shared__ double bsum[MS];
+    const long long np = c.npts;
+    const int nrows = c.ny * c.nz;
+    const int nw = (int)gridDim.x * WPB;
+    const cx<T>* twx = (const cx<T>*)c.twx;
+    cx<T>* S = (cx<T>*)a.S;
+    cx<T>* snap = (cx<T>*)a.snap;
+    auto issue = [&](int row, cx<T>* dst) {
+        for (int ch = lane; ch < MS * N; ch += 32) {
+            const int x = ch % N, m = ch / N;
+            cp_elem<T>(dst + m * LP + x + (x >> 3), S + (size_t)m * np + (size_t)row * N + x);
+        }
+    };
+    double acc[MS];
+#pragma unroll
+    for (int m = 0; m < MS; ++m) acc[m] = 0.0;
+    int row = (int)blockIdx.x * WPB + warp;
+    if (NBUF == 2) {
+        if (row < nrows) issue(row, mine);
+        cp_commit();
+    }
+    for (int it = 0; row < nrows; ++it, row += nw) {
+        cx<T>* cur = mine + (NBUF == 2 ? (it & 1) * TILE : 0);
+        if (NBUF == 2) {
+            const int nr = row + nw;
+            if (nr < nrows) issue(nr, mine + ((it + 1) & 1) * TILE);
+            cp_commit();
+            cp_wait<1>();
+        } else {
+            issue(row, cur);
+            cp_commit();
+            cp_wait<0>();
+        }
+        __syncwarp();
+        ct_fft<T, true, N, MS, 32, RT, 1>(cur, twx);
+        const int j = row % c.ny, k = row / c.ny;
+        for (int x = lane; x < N; x += 32) {
+            cx<T> v[MS];
+#pragma unroll
+            for (int m = 0; m < MS; ++m) v[m] = cur[m * LP + x + (x >> 3)];
+            const cx<T> eV = pot_phase<T>(c, x, j, k);
+            apply_se<T, MS>(c, v);
+            apply_sp<T, MS>(c, eV, v);
+            double w = c.wx[x];
+            if (c.dim >= 2) w *= c.wy[j];
+            if (c.dim >= 3) w *= c.wz[k];
+#pragma unroll
+            for (int m = 0; m < MS; ++m) {
+                acc[m] += w * ((double)v[m].x * (double)v[m].x + (double)v[m].y * (double)v[m].y);
+                cur[m * LP + x + (x >> 3)] = v[m];
+            }
+            if (snap) {
+#pragma unroll
+                for (int m = 0; m < MS; ++m) snap[(size_t)m * np + (size_t)row * N + x] = v[m];
+            }
+        }
+        __syncwarp();
+        ct_fft<T, false, N, MS, 32, RT, 1>(cur, twx);
+        for (int idx = lane; idx < MS * N; idx += 32) {
+            const int x = idx % N, m = idx / N;
+            S[(size_t)m * np + (size_t)row * N + x] = cur[m * LP + x + (x >> 3)];
+        }
+        __syncwarp();
+    }
+    cp_wait<0>();
+    asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
     block_sum<MS>(acc, red, bsum);
     if (threadIdx.x < MS) a.part[(size_t)blockIdx.x * MS + threadIdx.x] = bsum[threadIdx.x];
     finish_norms<MS>(c, a.part, a.counter, a.info, red);

@@ -47,12 +47,17 @@ enum { FGPE_KERNELS_AUTO = 0, FGPE_KERNELS_GENERIC = 1,
                                       step, even for short lines */
        FGPE_KERNELS_SINGLE_1D = 5, /* 1D: the single-block kernel whenever the
                                       line fits one block (200 KB) */
-       FGPE_KERNELS_CLUSTER_1D = 6 /* 1D: the N1 x N2 split on one 8-CTA
+       FGPE_KERNELS_CLUSTER_1D = 6,/* 1D: the N1 x N2 split on one 8-CTA
                                       thread-block cluster for a whole call,
                                       even for short lines (N1 and N2 multiples
                                       of 8; fgpe_create fails otherwise).  The
                                       default for split lines of N*M <= 10240
-                                      when the cluster fits. */ };
+                                      when the cluster fits. */
+       FGPE_KERNELS_WARP_ROW = 7   /* size-specialised kernels with the row pass
+                                      on one warp per x row (warp-private
+                                      shared memory, no block barriers in the
+                                      transforms) where the MS lines of a row
+                                      fit 16 KB; elsewhere as AUTO */ };
 
 /* Step flags for fgpe_step_ex. */
 enum {
