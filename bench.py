@@ -717,7 +717,10 @@ def time_to_ground_state(args):
         arms.append("learned")
     clocks = ClockSampler(0)
     clocks.start()
-    traces = {k: T.arm(k, tp, 256, net=infer, max_steps=args.tts_max_steps) for k in arms}
+    traces = {"plain": T.arm("plain", tp, 256, max_steps=args.tts_max_steps)}
+    e_ref = traces["plain"][-1][3]
+    for k in arms[1:]:
+        traces[k] = T.arm(k, tp, 256, net=infer, max_steps=args.tts_max_steps, e_ref=e_ref)
     clk = clocks.stop()
     e_star = min(tr[-1][3] for tr in traces.values())
     res = {}
@@ -746,7 +749,7 @@ def main():
     ap.add_argument("--precision", default=None, choices=["fp64", "fp32"],
                     help="arithmetic of the headline value (default fp64; the fp32 figure is added beside it)")
     ap.add_argument("--no-fp32", action="store_true", help="skip the FP32-bulk figure")
-    ap.add_argument("--kernels", default="auto", choices=["auto", "generic", "warp-row"],
+    ap.add_argument("--kernels", default="auto", choices=["auto", "generic", "warp-row", "block-row"],
                     help="kernel family of the timed propagators (fgpe_params.kernels)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="3d", choices=["3d", "q2d", "sweep", "golden1d", "tts", "fno", "tour"],
@@ -762,7 +765,7 @@ def main():
     ap.add_argument("--grid", type=int, default=0, help="with --capture --workload 3d: points per axis (192)")
     ap.add_argument("--observables", action="store_true", help="with --capture: also run ENERGY/RAD (k_obs)")
     ap.add_argument("--fno3d", default=None, help="with --workload tts: saved 3D network parameters (.npz)")
-    ap.add_argument("--tts-max-steps", type=int, default=40000, help="with --workload tts: steps per FP64 stage")
+    ap.add_argument("--tts-max-steps", type=int, default=60000, help="with --workload tts: steps per FP64 stage")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     args.precision_set = args.precision is not None

@@ -881,7 +881,7 @@ int fgpe_create(const fgpe_params* pin, fgpe_t** out) {
         if (gw > 0) {
             h->has_warp_row = true;
             h->warp_row_grid = gw;
-            h->warp_row = p.kernels == FGPE_KERNELS_WARP_ROW;
+            h->warp_row = p.kernels == FGPE_KERNELS_WARP_ROW || (p.kernels == FGPE_KERNELS_AUTO && !h->fp32);
         }
     }
     for (int a = 1; a < p.dim; ++a) {
@@ -1098,11 +1098,9 @@ int fgpe_step_ex(fgpe_t* h, int nsteps, int flags) {
         if (h->p.dim == 2) {
             DISPATCH(h, launch_col, h, 1, COL_SCALE | COL_FWD | COL_KOP | COL_INV);
         } else {
-            // KE in the z pass; SO coupling (a function of kx, ky only)
-            // after the inverse z transform, in the inverse y pass
             DISPATCH(h, launch_col, h, 1, COL_SCALE | COL_FWD);
-            DISPATCH(h, launch_col, h, 2, COL_FWD | COL_KE | COL_INV);
-            DISPATCH(h, launch_col, h, 1, COL_SOC | COL_INV);
+            DISPATCH(h, launch_col, h, 2, COL_FWD | COL_KOP | COL_INV);
+            DISPATCH(h, launch_col, h, 1, COL_INV);
         }
         DISPATCH(h, launch_row, h, ROW_FULL, sn);
     };
@@ -1291,7 +1289,7 @@ int fgpe_set_kernels(fgpe_t* h, int kernels) {
     if (h->bulk) { CK(cudaStreamSynchronize(h->st)); cudaGraphExecDestroy(h->bulk); h->bulk = nullptr; }
     const bool fast = kernels != FGPE_KERNELS_GENERIC;
     h->fast_row = fast && h->has_fast_row && kernels != FGPE_KERNELS_FAST_COL_ONLY;
-    h->warp_row = h->has_warp_row && kernels == FGPE_KERNELS_WARP_ROW;
+    h->warp_row = h->has_warp_row && (kernels == FGPE_KERNELS_WARP_ROW || (kernels == FGPE_KERNELS_AUTO && !h->fp32));
     for (int a = 0; a < 3; ++a) h->fast_col[a] = fast && h->has_fast_col[a] && kernels != FGPE_KERNELS_FAST_ROW_ONLY;
     return FGPE_OK;
 }

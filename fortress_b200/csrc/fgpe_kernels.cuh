@@ -6,10 +6,8 @@
 // step (cgpe1d.f90:434-441, 470-472) is then
 //   2D: col pass   (y)  : load S * scale/N, F_y, KE, SOC, F_y^-1, store
 //       row pass   (x)  : load, F_x^-1, SE, SP, NORMC partials, F_x, store
-//   3D: col pass y (F_y, with scale/N), col pass z (F_z, KE, F_z^-1),
-//       col pass y (SOC, F_y^-1), row pass x as above; SOC depends on
-//       (kx, ky) only, so it commutes with the z transform and follows KE
-//       in the inverse y pass
+//   3D: col pass y (F_y, with scale/N), col pass z (F_z, KE, SOC, F_z^-1),
+//       col pass y (F_y^-1), row pass x as above
 // so a 2D step streams the spinor through HBM twice and a 3D step four times.
 // The row pass's last block finishes the NORMC reduction in a fixed order and
 // publishes norms and the next scale (no host round trip).

@@ -22,10 +22,8 @@ enum {
 
 enum { ROW_FULL = 0, ROW_FWD = 1, ROW_INV = 2 };
 // Column-pass work: COL_KE and COL_SOC act in k-space between the forward
-// and inverse transforms of the pass.  In 3D the SO-coupling factor depends
-// on (kx, ky) only, so it commutes with the z transform and runs in the
-// inverse y pass, after the z pass has applied KE (cgpe3d.f90:452-454 keep
-// the order KE then SOC).
+// and inverse transforms of the pass (KE before SOC, cgpe3d.f90:452-454).
+// Every step applies both in one pass (2D: the y pass; 3D: the z pass).
 enum { COL_SCALE = 1, COL_FWD = 2, COL_KE = 4, COL_INV = 8, COL_SOC = 16, COL_KOP = COL_KE | COL_SOC };
 enum { OBS_FULL = 0, OBS_NORMS = 1, OBS_NORMALIZE = 2 };
 enum { OP_KE = 1, OP_SOC = 2, OP_SE = 3, OP_SP = 4, OP_SCALE = 5 };

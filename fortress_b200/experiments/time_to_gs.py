@@ -158,12 +158,13 @@ class Clock:
         return time.perf_counter() - self.t0
 
 
-def run_to(prop, clock, trace, label, max_steps, stop_rule=None, dt=1e-3):
+def run_to(prop, clock, trace, label, max_steps, stop_rule=None, dt=1e-3, settle=None):
     """STP-step blocks with ENERGY and CONV after each, appending
-    (label, step, wall, E, CONV, CONV_EN) to trace; stops at max_steps or
-    when stop_rule(conv, conv_en) holds."""
+    (label, step, wall, E, CONV, CONV_EN) to trace; stops at max_steps, when
+    stop_rule(conv, conv_en) holds, or, with settle = (E_ref, checks), once
+    |E - E_ref| <= TOL_REL/2 |E_ref| has held for that many checks."""
     en_old = prop.observables()[0]
-    done = 0
+    done, held = 0, 0
     while done < max_steps:
         prop.step(STP)
         done += STP
@@ -174,6 +175,10 @@ def run_to(prop, clock, trace, label, max_steps, stop_rule=None, dt=1e-3):
         trace.append((label, done, clock(), en, c, ce))
         if stop_rule is not None and stop_rule(c, ce):
             break
+        if settle is not None:
+            held = held + 1 if abs(en - settle[0]) <= 0.5 * TOL_REL * abs(settle[0]) else 0
+            if held >= settle[1]:
+                break
     return done
 
 
@@ -205,8 +210,10 @@ def prolong(phi64_dev, n):
     return (torch.fft.ifftn(big, dim=(1, 2, 3)) * (n / m) ** 3).contiguous()
 
 
-def arm(kind, point, n, clock_state=None, net=None, max_steps=60000, fp32_tol=1e-6):
-    """One arm on the n^3 grid; returns its trace."""
+def arm(kind, point, n, clock_state=None, net=None, max_steps=60000, fp32_tol=1e-6, e_ref=None):
+    """One arm on the n^3 grid; returns its trace.  e_ref: the plain arm's
+    final energy; the other arms' FP64 stages stop once they have held
+    within half the tolerance of it for 20 checks."""
     import fortress_b200 as F
     import torch
     trace = []
@@ -245,7 +252,7 @@ def arm(kind, point, n, clock_state=None, net=None, max_steps=60000, fp32_tol=1e
     p64.normt()
     del guess
     trace.append(("switch", 0, clock(), p64.observables()[0], float("nan"), float("nan")))
-    run_to(p64, clock, trace, "fp64", max_steps)
+    run_to(p64, clock, trace, "fp64", max_steps, settle=(e_ref, 20) if e_ref is not None else None)
     p64.close()
     return trace
 
@@ -271,12 +278,12 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--train", type=int, default=192)
     ap.add_argument("--n-train", type=int, default=64)
-    ap.add_argument("--gen-steps", type=int, default=8000)
+    ap.add_argument("--gen-steps", type=int, default=30000)
     ap.add_argument("--epochs", type=int, default=60)
     ap.add_argument("--batch", type=int, default=4)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--n", type=int, default=256)
-    ap.add_argument("--max-steps", type=int, default=40000)
+    ap.add_argument("--max-steps", type=int, default=60000)
     ap.add_argument("--arms", default="plain,learned,learned64,coarse")
     ap.add_argument("--out", default=None)
     args = ap.parse_args()
@@ -301,8 +308,13 @@ def main():
     from fortress_b200 import fno3d as F3
     infer = F3.FNO3(args.n, 1, params=params_np, train=False)
     traces = {}
-    for kind in args.arms.split(","):
-        traces[kind] = arm(kind, tp, args.n, net=infer, max_steps=args.max_steps)
+    kinds = args.arms.split(",")
+    kinds = (["plain"] if "plain" in kinds else []) + [k for k in kinds if k != "plain"]
+    e_ref = None
+    for kind in kinds:
+        traces[kind] = arm(kind, tp, args.n, net=infer, max_steps=args.max_steps, e_ref=e_ref)
+        if kind == "plain":
+            e_ref = traces[kind][-1][3]
         last = traces[kind][-1]
         print(json.dumps({"stage": "arm", "arm": kind, "wall": last[2], "E_final": last[3],
                           "fp64_steps": last[1]}), flush=True)

@@ -50,7 +50,7 @@ def make_params(dim, spin, n, d, dt, imag_time, tau, gamma=(0.0, 0.0, 0.0),
         p.alpha[i] = float(alpha[i])
     p.precision = _abi.FGPE_FP32 if str(precision).lower() in ("fp32", "float32", "1") else _abi.FGPE_FP64
     p.kernels = {"auto": 0, "generic": 1, "fast-row": 2, "fast-col": 3, "split-1d": 4, "single-1d": 5, "cluster-1d": 6,
-                 "warp-row": 7}[kernels]
+                 "warp-row": 7, "block-row": 8}[kernels]
     p.mag = float(mag)
     return p
 
@@ -194,7 +194,7 @@ class Propagator:
 
     def set_kernels(self, kernels):
         self._ck(self._L.fgpe_set_kernels(self._h, {"auto": 0, "generic": 1, "fast-row": 2, "fast-col": 3,
-                                                    "warp-row": 7}[kernels]))
+                                                    "warp-row": 7, "block-row": 8}[kernels]))
 
     def save(self, path, step=0, user=None):
         """Full-precision checkpoint (fgpe_checkpoint_save); user: up to 8 floats."""

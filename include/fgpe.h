@@ -53,11 +53,14 @@ enum { FGPE_KERNELS_AUTO = 0, FGPE_KERNELS_GENERIC = 1,
                                       of 8; fgpe_create fails otherwise).  The
                                       default for split lines of N*M <= 10240
                                       when the cluster fits. */
-       FGPE_KERNELS_WARP_ROW = 7   /* size-specialised kernels with the row pass
+       FGPE_KERNELS_WARP_ROW = 7,  /* size-specialised kernels with the row pass
                                       on one warp per x row (warp-private
                                       shared memory, no block barriers in the
                                       transforms) where the MS lines of a row
-                                      fit 16 KB; elsewhere as AUTO */ };
+                                      fit 16 KB, in either precision; AUTO
+                                      takes this row pass for FP64 */
+       FGPE_KERNELS_BLOCK_ROW = 8  /* size-specialised kernels with the
+                                      block-tiled row pass everywhere */ };
 
 /* Step flags for fgpe_step_ex. */
 enum {

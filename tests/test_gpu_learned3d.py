@@ -43,7 +43,7 @@ def test_learned_guess_reaches_the_ground_state_in_fewer_steps():
     from fortress_b200.experiments import time_to_gs as T
     pts = T.box_points(24, seed=5)
     held = T.box_points(2, seed=6)
-    states, conv = T.ground_states(pts, N, 12000, precision="fp32", chunk=24)
+    states, conv = T.ground_states(pts, N, 20000, precision="fp32", chunk=24)
     assert np.all(np.isfinite(states))
     net, hist = T.train(pts, states, N, epochs=40, batch=4, lr=3e-3, width=8, modes=6, layers=3, hidden=32)
     assert hist[-1] < 0.2 * hist[0], hist
@@ -54,13 +54,13 @@ def test_learned_guess_reaches_the_ground_state_in_fewer_steps():
         a = F.Propagator(**p)
         a.set_state(T.gaussian_start(N))
         a.normt()
-        ta = _run(a, 40000)
+        ta = _run(a, 60000)
         a.close()
         guess = T.learned_guess_device(infer, pt, N)
         b = F.Propagator(**p)
         b.set_state_device(guess.data_ptr())
         b.normt()
-        tb = _run(b, 40000)
+        tb = _run(b, 60000)
         b.close()
         e_star = min(ta[-1][1], tb[-1][1])
         sa, sb = _steps_to(ta, e_star), _steps_to(tb, e_star)

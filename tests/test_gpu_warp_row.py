@@ -1,5 +1,6 @@
-"""Row pass with one warp per x row (FGPE_KERNELS_WARP_ROW) against the block
-row kernel and the oracle: the same per-element arithmetic, so real-time
+"""Row pass with one warp per x row (FGPE_KERNELS_WARP_ROW; the automatic
+choice for FP64) against the block row kernel (FGPE_KERNELS_BLOCK_ROW) and
+the oracle: the same per-element arithmetic, so real-time
 states are bitwise equal and imaginary-time states differ only through the
 NORMC summation order; both follow the oracle at the parity bars."""
 import numpy as np
@@ -34,7 +35,7 @@ def test_warp_row_matches_block_row_and_oracle(case):
     orc = O.Oracle(**oracle_kwargs(q))
     phi = initial_state(orc, seed=5)
     orc.set_state(phi)
-    a = F.Propagator(**p)
+    a = F.Propagator(**p, kernels="block-row")
     b = F.Propagator(**p, kernels="warp-row")
     for x in (a, b):
         x.set_state(phi)
