@@ -408,6 +408,7 @@ __global__ void __launch_bounds__(TH, FGPE_COL_MINB) k_col_fast(StepConst c, Col
     constexpr int NCH = MS * N * CPL;
     extern __shared__ __align__(16) unsigned char smraw[];
     cx<T>* bufs = (cx<T>*)smraw;
+    __shared__ cx<T> usoc[TX * MS * MS];     // per-column SO-coupling matrices (z pass)
     const long long np = c.npts;
     const int nxt = c.nx / TX;
     const int nother = (int)a.n_other;
@@ -472,6 +473,28 @@ __global__ void __launch_bounds__(TH, FGPE_COL_MINB) k_col_fast(StepConst c, Col
         }
         if (a.flags & COL_FWD) ct_fft<T, false, N, MS * TX, TH, CT>(cur, tw);
         if (a.flags & COL_KOP) {
+            // z lines: (kx, ky) is fixed along each line of the tile, so the
+            // SO-coupling exponential is one MS x MS matrix per tile column,
+            // built here by applying apply_soc to the unit vectors and then
+            // applied to every point as one matrix-vector product
+            const bool zmat = a.axis == 2 && (a.flags & COL_SOC);
+            if (zmat) {
+                if (threadIdx.x < TX * MS) {
+                    const int t = threadIdx.x / MS, j = threadIdx.x - (threadIdx.x / MS) * MS;
+                    cx<T> u[MS];
+#pragma unroll
+                    for (int m = 0; m < MS; ++m) u[m] = mk<T>(m == j ? (T)1 : (T)0, (T)0);
+                    const int ixt = c.fx[x0 + t], iyt = c.fy[oth];
+                    apply_soc<T, MS>(c, c.kx[ixt], c.ky[iyt], u);
+                    // the kx, ky part of KE, exp(-i CDT (kx^2 + ky^2)), is a
+                    // scalar along the line: folded into the matrix
+                    const cx<T> f = (a.flags & COL_KE) ? cmul(((const cx<T>*)c.kex)[ixt], ((const cx<T>*)c.key)[iyt])
+                                                        : mk<T>((T)1, (T)0);
+#pragma unroll
+                    for (int r = 0; r < MS; ++r) usoc[(t * MS + r) * MS + j] = cmul(u[r], f);
+                }
+                __syncthreads();
+            }
             for (int p = threadIdx.x; p < N * TX; p += TH) {
                 const int t = p % TX, e = p / TX;
                 const int ix = c.fx[x0 + t];
@@ -485,8 +508,31 @@ __global__ void __launch_bounds__(TH, FGPE_COL_MINB) k_col_fast(StepConst c, Col
 #pragma unroll
                     for (int m = 0; m < MS; ++m) v[m] = cscale(v[m], fac[m]);
                 }
-                if (a.flags & COL_KE) apply_ke<T, MS>(c, ix, iy, iz, v);
-                if (a.flags & COL_SOC) apply_soc<T, MS>(c, c.kx[ix], c.ky[iy], v);
+                if (zmat) {
+                    if (a.flags & COL_KE) {
+                        // the kz part, exp(-i CDT (kz^2 - 2 L GAMMAZ kz)) per component
+                        const cx<T>* kez = (const cx<T>*)c.kez;
+#pragma unroll
+                        for (int m = 0; m < MS; ++m) v[m] = cmul(v[m], kez[m * c.nz + iz]);
+                    }
+                } else if (a.flags & COL_KE) {
+                    apply_ke<T, MS>(c, ix, iy, iz, v);
+                }
+                if (zmat) {
+                    const cx<T>* U = usoc + t * MS * MS;
+                    cx<T> w[MS];
+#pragma unroll
+                    for (int r = 0; r < MS; ++r) {
+                        cx<T> acc = cmul(U[r * MS], v[0]);
+#pragma unroll
+                        for (int q = 1; q < MS; ++q) acc = cmac(acc, U[r * MS + q], v[q]);
+                        w[r] = acc;
+                    }
+#pragma unroll
+                    for (int m = 0; m < MS; ++m) v[m] = w[m];
+                } else if (a.flags & COL_SOC) {
+                    apply_soc<T, MS>(c, c.kx[ix], c.ky[iy], v);
+                }
 #pragma unroll
                 for (int m = 0; m < MS; ++m) cur[(m * LPN + e + (e >> 3)) * TX + t] = v[m];
             }
