@@ -700,13 +700,15 @@ def time_to_ground_state(args):
     time_to_gs): plain FP64 from INITIALIZE's seeded Gaussian (the
     reference's method); coarse (64^3 FP64 solve, spectral prolongation,
     FP32 to its stop rule, then FP64); learned (the trained 3D network's
-    guess, FP32, then FP64) when --fno3d names a saved parameter file."""
+    guess, FP32, then FP64) and learned_coarse (the guess on 64^3 as the
+    coarse solve's start, then as coarse) when --fno3d names a saved
+    parameter file."""
     import numpy as np
     import torch
     from fortress_b200.experiments import time_to_gs as T
     tp = T.target_point()
     arms = ["plain", "coarse"]
-    infer = None
+    infer = infer64 = None
     if args.fno3d:
         from fortress_b200 import fno3d as F3
         pz = dict(np.load(args.fno3d))
@@ -714,13 +716,14 @@ def time_to_ground_state(args):
         M = pz["Rr0"].shape[-1]
         layers = sum(1 for k in pz if k.startswith("Rr"))
         infer = F3.FNO3(256, 1, params=pz, width=W, modes=M, layers=layers, hidden=pz["Q1"].shape[0], train=False)
-        arms.append("learned")
+        infer64 = F3.FNO3(64, 1, params=pz, width=W, modes=M, layers=layers, hidden=pz["Q1"].shape[0], train=False)
+        arms += ["learned", "learned_coarse"]
     clocks = ClockSampler(0)
     clocks.start()
     traces = {"plain": T.arm("plain", tp, 256, max_steps=args.tts_max_steps)}
     e_ref = traces["plain"][-1][3]
     for k in arms[1:]:
-        traces[k] = T.arm(k, tp, 256, net=infer, max_steps=args.tts_max_steps, e_ref=e_ref)
+        traces[k] = T.arm(k, tp, 256, net=infer, max_steps=args.tts_max_steps, e_ref=e_ref, coarse_net=infer64)
     clk = clocks.stop()
     e_star = min(tr[-1][3] for tr in traces.values())
     res = {}

@@ -21,6 +21,9 @@ is needed:
              stop rule at 1e-8), spectrally prolonged to 256^3 (zero padding
              of the 64^3 spectrum), then FP32 and FP64 as in "learned" (the
              coarse-to-fine gain without learning).
+  learned_coarse  the network's guess on the 64^3 grid as the start of the
+             coarse solve, then as "coarse" (the network's gain on top of the
+             coarse-to-fine method).
 
 The target parameter point is held out of the training set (the training
 points are drawn from the box with seed 5 and none coincides with it).
@@ -210,7 +213,7 @@ def prolong(phi64_dev, n):
     return (torch.fft.ifftn(big, dim=(1, 2, 3)) * (n / m) ** 3).contiguous()
 
 
-def arm(kind, point, n, clock_state=None, net=None, max_steps=60000, fp32_tol=1e-6, e_ref=None):
+def arm(kind, point, n, clock_state=None, net=None, max_steps=60000, fp32_tol=1e-6, e_ref=None, coarse_net=None):
     """One arm on the n^3 grid; returns its trace.  e_ref: the plain arm's
     final energy; the other arms' FP64 stages stop once they have held
     within half the tolerance of it for 20 checks."""
@@ -228,9 +231,12 @@ def arm(kind, point, n, clock_state=None, net=None, max_steps=60000, fp32_tol=1e
         return trace
     if kind in ("learned", "learned64"):
         guess = learned_guess_device(net, point, n)
-    else:   # coarse: 64^3 FP64 solve to the stop rule at 1e-8, then prolong
+    else:   # coarse (learned_coarse): 64^3 FP64 solve to the stop rule at 1e-8, then prolong
         pc = F.Propagator(**params(point, 64, "fp64"))
-        pc.set_state(gaussian_start(64))
+        if kind == "learned_coarse":
+            pc.set_state_device(learned_guess_device(coarse_net, point, 64).data_ptr())
+        else:
+            pc.set_state(gaussian_start(64))
         pc.normt()
         run_to(pc, clock, trace, "coarse64", 200000, stop_rule=lambda c, ce: c <= 1e-8 or ce <= 1e-8)
         buf = torch.empty((3, 64, 64, 64), dtype=torch.complex128, device="cuda")
@@ -284,35 +290,42 @@ def main():
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--max-steps", type=int, default=60000)
-    ap.add_argument("--arms", default="plain,learned,learned64,coarse")
+    ap.add_argument("--arms", default="plain,learned,learned64,coarse,learned_coarse")
+    ap.add_argument("--params", default=None, help="trained network parameters (.npz): skip data and training")
     ap.add_argument("--out", default=None)
     args = ap.parse_args()
     out = args.out or os.environ.get("FGPE_BENCH_OUT") or "."
     os.makedirs(out, exist_ok=True)
     import torch
-    pts = box_points(args.train, seed=5)
     tp = target_point()
-    t0 = time.perf_counter()
-    states, conv = ground_states(pts, args.n_train, args.gen_steps)
-    print(json.dumps({"stage": "data", "count": len(pts), "grid": args.n_train, "steps": args.gen_steps,
-                      "seconds": time.perf_counter() - t0, "conv_median": float(np.median(conv)),
-                      "conv_max": float(conv.max())}), flush=True)
-    t0 = time.perf_counter()
-    net, hist = train(pts, states, args.n_train, args.epochs, args.batch, args.lr)
-    print(json.dumps({"stage": "train", "epochs": args.epochs, "seconds": time.perf_counter() - t0,
-                      "loss_first": hist[0], "loss_last": hist[-1]}), flush=True)
-    params_np = net.params_numpy()
-    np.savez(os.path.join(out, "fno3d_params.npz"), **params_np)
-    del net, states
-    torch.cuda.empty_cache()
+    if args.params:
+        params_np = {k: np.asarray(v, np.float64) for k, v in np.load(args.params).items()}
+    else:
+        pts = box_points(args.train, seed=5)
+        t0 = time.perf_counter()
+        states, conv = ground_states(pts, args.n_train, args.gen_steps)
+        print(json.dumps({"stage": "data", "count": len(pts), "grid": args.n_train, "steps": args.gen_steps,
+                          "seconds": time.perf_counter() - t0, "conv_median": float(np.median(conv)),
+                          "conv_max": float(conv.max())}), flush=True)
+        t0 = time.perf_counter()
+        net, hist = train(pts, states, args.n_train, args.epochs, args.batch, args.lr)
+        print(json.dumps({"stage": "train", "epochs": args.epochs, "seconds": time.perf_counter() - t0,
+                          "loss_first": hist[0], "loss_last": hist[-1]}), flush=True)
+        params_np = net.params_numpy()
+        np.savez(os.path.join(out, "fno3d_params.npz"), **{k: v.astype(np.float32) for k, v in params_np.items()})
+        del net, states
+        torch.cuda.empty_cache()
     from fortress_b200 import fno3d as F3
-    infer = F3.FNO3(args.n, 1, params=params_np, train=False)
+    shape = dict(width=params_np["P"].shape[0], modes=params_np["Rr0"].shape[-1], hidden=params_np["Q1"].shape[0],
+                 layers=sum(1 for k in params_np if k.startswith("Rr")))
+    infer = F3.FNO3(args.n, 1, params=params_np, train=False, **shape)
+    infer64 = F3.FNO3(64, 1, params=params_np, train=False, **shape)
     traces = {}
     kinds = args.arms.split(",")
     kinds = (["plain"] if "plain" in kinds else []) + [k for k in kinds if k != "plain"]
     e_ref = None
     for kind in kinds:
-        traces[kind] = arm(kind, tp, args.n, net=infer, max_steps=args.max_steps, e_ref=e_ref)
+        traces[kind] = arm(kind, tp, args.n, net=infer, max_steps=args.max_steps, e_ref=e_ref, coarse_net=infer64)
         if kind == "plain":
             e_ref = traces[kind][-1][3]
         last = traces[kind][-1]
@@ -324,9 +337,10 @@ def main():
         t = time_to(tr, e_star)
         res["arms"][kind] = {"time_to_tol_s": t[1] if t else None, "steps": t[0] if t else None,
                              "E_final": tr[-1][3], "E_final_minus_Estar_rel": (tr[-1][3] - e_star) / abs(e_star)}
-    if res["arms"].get("plain", {}).get("time_to_tol_s") and res["arms"].get("learned", {}).get("time_to_tol_s"):
-        res["speedup_learned_fp32_vs_plain_fp64"] = res["arms"]["plain"]["time_to_tol_s"] / \
-            res["arms"]["learned"]["time_to_tol_s"]
+    plain = res["arms"].get("plain", {}).get("time_to_tol_s")
+    for k, v in res["arms"].items():
+        if k != "plain" and plain and v.get("time_to_tol_s"):
+            v["speedup_vs_plain_fp64"] = plain / v["time_to_tol_s"]
     with open(os.path.join(out, "time_to_gs.json"), "w") as f:
         json.dump({"result": res, "traces": traces}, f)
     print(json.dumps(res), flush=True)

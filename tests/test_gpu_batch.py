@@ -152,7 +152,10 @@ def test_grouped_batch_matches_individual(F):
         tol = 1e-13 if p["precision"] == "fp64" else 2e-6
         sa, sb = b[i].state(), singles[i].state()
         assert np.abs(sa - sb).max() <= tol * np.abs(sb).max(), (i, float(np.abs(sa - sb).max()))
-        assert np.allclose(b[i].normc(), singles[i].normc(), rtol=1e-12, atol=0), i
+        # reductions are FP64 in both precisions, of states that agree to tol
+        rt = 1e-12 if p["precision"] == "fp64" else 1e-6
+        assert np.allclose(b[i].normc(), singles[i].normc(), rtol=rt, atol=0), i
         en, mu, mz, rms = singles[i].observables()
-        assert abs(obs[i]["en"] - en) <= 1e-12 * abs(en) and np.allclose(obs[i]["rms"], rms, rtol=1e-12), i
-        assert abs(obs[i]["conv"] - singles[i].conv()) <= 1e-10 * max(singles[i].conv(), 1e-12), i
+        assert abs(obs[i]["en"] - en) <= rt * abs(en) and np.allclose(obs[i]["rms"], rms, rtol=rt), i
+        assert abs(obs[i]["conv"] - singles[i].conv()) <= (1e-10 if p["precision"] == "fp64" else 1e-4) * \
+            max(singles[i].conv(), 1e-12), i
