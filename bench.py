@@ -668,6 +668,9 @@ def sweep(args):
         b[i].set_state(gaussian_nd(p))
         b[i].normt()
     tune = b.autotune(trial_steps=4, cache_path=os.path.join(out_dir(), "autotune_cache.txt"))
+    if args.batch_mode != "auto":
+        b.mode(grouped=args.batch_mode == "grouped")
+        b.config(tune[0], tune[1])
     npts = sum(int(np.prod(p["n"])) for p in insts)
     b.step(max(args.warmup, 4))
     clocks.start()
@@ -683,7 +686,7 @@ def sweep(args):
            "dtype": "c128" if prec == "fp64" else "c64", "data": "synthetic (seeded parameter box, seed 4)",
            "config": {"workload": "sweep-512-ragged-q2d-spin1-imag", "instances": len(insts),
                       "sizes": sorted(set(p["n"][0] for p in insts)), "precision": prec,
-                      "autotuned": {"width": tune[0], "steps_per_graph": tune[1]},
+                      "autotuned": {"width": tune[0], "steps_per_graph": tune[1]}, "batch_mode": args.batch_mode,
                       "l2": "batch state larger than L2"},
            "roofline": {"bound": "hbm", "kernel": "whole batch step", "achieved": alg / (el / steps) / 1e9,
                         "peak": peak, "unit": "GB/s", "frac": alg / (el / steps) / 1e9 / peak,
@@ -768,6 +771,8 @@ def main():
     ap.add_argument("--grid", type=int, default=0, help="with --capture --workload 3d: points per axis (192)")
     ap.add_argument("--observables", action="store_true", help="with --capture: also run ENERGY/RAD (k_obs)")
     ap.add_argument("--fno3d", default=None, help="with --workload tts: saved 3D network parameters (.npz)")
+    ap.add_argument("--batch-mode", default="auto", choices=["auto", "grouped", "branches"],
+                    help="with --workload sweep: the autotuner's choice, or force grouped / per-instance branches")
     ap.add_argument("--tts-max-steps", type=int, default=60000, help="with --workload tts: steps per FP64 stage")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

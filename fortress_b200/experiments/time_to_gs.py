@@ -292,6 +292,11 @@ def main():
     ap.add_argument("--max-steps", type=int, default=60000)
     ap.add_argument("--arms", default="plain,learned,learned64,coarse,learned_coarse")
     ap.add_argument("--params", default=None, help="trained network parameters (.npz): skip data and training")
+    ap.add_argument("--width", type=int, default=16)
+    ap.add_argument("--modes", type=int, default=8)
+    ap.add_argument("--layers", type=int, default=4)
+    ap.add_argument("--hidden", type=int, default=64)
+    ap.add_argument("--data", default=None, help="reuse training states saved by an earlier run (.npy)")
     ap.add_argument("--out", default=None)
     args = ap.parse_args()
     out = args.out or os.environ.get("FGPE_BENCH_OUT") or "."
@@ -303,12 +308,17 @@ def main():
     else:
         pts = box_points(args.train, seed=5)
         t0 = time.perf_counter()
-        states, conv = ground_states(pts, args.n_train, args.gen_steps)
-        print(json.dumps({"stage": "data", "count": len(pts), "grid": args.n_train, "steps": args.gen_steps,
-                          "seconds": time.perf_counter() - t0, "conv_median": float(np.median(conv)),
-                          "conv_max": float(conv.max())}), flush=True)
+        if args.data:
+            states = np.load(args.data)
+        else:
+            states, conv = ground_states(pts, args.n_train, args.gen_steps)
+            np.save(os.path.join(out, "train_states.npy"), states)
+            print(json.dumps({"stage": "data", "count": len(pts), "grid": args.n_train, "steps": args.gen_steps,
+                              "seconds": time.perf_counter() - t0, "conv_median": float(np.median(conv)),
+                              "conv_max": float(conv.max())}), flush=True)
         t0 = time.perf_counter()
-        net, hist = train(pts, states, args.n_train, args.epochs, args.batch, args.lr)
+        net, hist = train(pts, states, args.n_train, args.epochs, args.batch, args.lr, width=args.width,
+                          modes=args.modes, layers=args.layers, hidden=args.hidden)
         print(json.dumps({"stage": "train", "epochs": args.epochs, "seconds": time.perf_counter() - t0,
                           "loss_first": hist[0], "loss_last": hist[-1]}), flush=True)
         params_np = net.params_numpy()
