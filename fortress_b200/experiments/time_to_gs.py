@@ -18,9 +18,10 @@ is needed:
              its own stop rule (CONV or CONV_EN <= 1e-6), then FP64.
   learned64  the same guess, FP64 throughout (the network's own gain).
   coarse     no network: the plain start solved on the 64^3 grid (FP64, to the
-             stop rule at 1e-8), spectrally prolonged to 256^3 (zero padding
-             of the 64^3 spectrum), then FP32 and FP64 as in "learned" (the
-             coarse-to-fine gain without learning).
+             stop rule at 1e-8), spectrally prolonged to 256^3 (the library's
+             FFT on 64^3, zero padding of the spectrum, its BFT on 256^3),
+             then FP32 and FP64 as in "learned" (the coarse-to-fine gain
+             without learning).
   learned_coarse  the network's guess on the 64^3 grid as the start of the
              coarse solve, then as "coarse" (the network's gain on top of the
              coarse-to-fine method).
@@ -195,22 +196,19 @@ def learned_guess_device(net, point, n):
     return torch.complex(o[0::2].double(), o[1::2].double()).contiguous()   # [m][z][y][x] = PHI layout
 
 
-def prolong(phi64_dev, n):
-    """Spectral prolongation of a device PHI array [m][z][y][x] from its grid
-    to n^3 (zero padding of the spectrum; same box, so the values scale by
-    nothing once the FFT normalisations cancel)."""
+def pad_spectrum(spec, n):
+    """Zero padding of a natural-order device spectrum [m][z][y][x] of an
+    m^3 grid to n^3 (the prolongation's only step outside the library's
+    transforms: a device copy of the kept frequencies)."""
     import torch
-    m = phi64_dev.shape[-1]
-    spec = torch.fft.fftn(phi64_dev, dim=(1, 2, 3))
+    m = spec.shape[-1]
     h = m // 2
-    big = torch.zeros((3, n, n, n), dtype=spec.dtype, device=spec.device)
-    idx = list(range(h)) + list(range(n - h, n))
-    src = list(range(h)) + list(range(m - h, m))
-    ii = torch.tensor(idx, device=spec.device)
-    ss = torch.tensor(src, device=spec.device)
+    big = torch.zeros((spec.shape[0], n, n, n), dtype=spec.dtype, device=spec.device)
+    ii = torch.tensor(list(range(h)) + list(range(n - h, n)), device=spec.device)
+    ss = torch.tensor(list(range(h)) + list(range(m - h, m)), device=spec.device)
     big[:, ii[:, None, None], ii[None, :, None], ii[None, None, :]] = \
         spec[:, ss[:, None, None], ss[None, :, None], ss[None, None, :]]
-    return (torch.fft.ifftn(big, dim=(1, 2, 3)) * (n / m) ** 3).contiguous()
+    return big
 
 
 def arm(kind, point, n, clock_state=None, net=None, max_steps=60000, fp32_tol=1e-6, e_ref=None, coarse_net=None):
@@ -239,15 +237,22 @@ def arm(kind, point, n, clock_state=None, net=None, max_steps=60000, fp32_tol=1e
             pc.set_state(gaussian_start(64))
         pc.normt()
         run_to(pc, clock, trace, "coarse64", 200000, stop_rule=lambda c, ce: c <= 1e-8 or ce <= 1e-8)
+        # spectral prolongation with the library's transforms: the coarse
+        # state's unnormalised spectrum (FFT, natural order), zero-padded to
+        # n^3, taken back by the fine grid's BFT; NORMT then fixes the scale
+        pc.FFT()
         buf = torch.empty((3, 64, 64, 64), dtype=torch.complex128, device="cuda")
         pc.get_state_device(buf.data_ptr())
         pc.close()
-        guess = prolong(buf, n)
+        guess = pad_spectrum(buf, n)
+        del buf
     torch.cuda.synchronize()
     trace.append(("guess", 0, clock(), float("nan"), float("nan"), float("nan")))
     if kind != "learned64":
         p32 = F.Propagator(**params(point, n, "fp32"))
         p32.set_state_device(guess.data_ptr())
+        if kind in ("coarse", "learned_coarse"):
+            p32.BFT()
         p32.normt()
         run_to(p32, clock, trace, "fp32", max_steps, stop_rule=lambda c, ce: c <= fp32_tol or ce <= fp32_tol)
         buf = torch.empty_like(guess)
