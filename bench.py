@@ -172,11 +172,11 @@ def measured_peaks():
 
 
 def profile_figures(workload, precision, kernel):
-    """Per-launch DRAM traffic and FP64 operation count of a kernel, from the
-    committed ncu summaries (profiles/traffic.json: dram__bytes_read.sum +
-    dram__bytes_write.sum, and the FP64 flops from the dadd/dmul/dfma
-    instruction counts, per launch, scaled to the bench grid where the
-    capture ran on a smaller one).  (None, None) when not captured."""
+    """Per-launch DRAM traffic and FP64 pipe utilisation of a kernel, from
+    the committed ncu summaries (profiles/traffic.json: dram__bytes_read.sum
+    + dram__bytes_write.sum per launch, scaled to the bench grid where the
+    capture ran on a smaller one, and sm__pipe_fp64_cycles_active in % of its
+    peak).  (None, None) when not captured."""
     path = os.path.join(ROOT, "profiles", "traffic.json")
     try:
         with open(path) as f:
@@ -187,7 +187,7 @@ def profile_figures(workload, precision, kernel):
     if e is None:
         return None, None
     if isinstance(e, dict):
-        return e.get("dram_bytes"), e.get("fp64_flops")
+        return e.get("dram_bytes"), e.get("fp64_pipe_pct")
     return e, None
 
 
@@ -277,6 +277,22 @@ def capture(args):
         return
     if args.workload == "tour":
         return kernel_tour(args)
+    if args.workload == "sweep":
+        # a reduced phase-diagram batch in the grouped mode: 32 instances of
+        # the seeded box, warmup + steps grouped steps
+        from fortress_b200.batch import Batch
+        insts = sweep_instances(count=32, precision=args.precision if args.precision_set else "fp32")
+        b = Batch(insts)
+        for i, p in enumerate(insts):
+            b[i].set_state(gaussian_nd(p))
+            b[i].normt()
+        b.mode(grouped=True)
+        b.config(32, 4)
+        b.step(args.warmup + args.steps)
+        obs = b.observables(with_conv=False)
+        assert all(np.isfinite(o["en"]) for o in obs)
+        print(json.dumps({"capture": "sweep-grouped-32", "steps": args.warmup + args.steps}))
+        return
     w = WORKLOADS[args.workload]
     if w is D3:
         g = args.grid or 192
@@ -443,14 +459,23 @@ def roofline(w, precision, kms, kn, peak, peak_kind, fp64_peak):
     per_launch_ms = kms[dom] / max(kn[dom], 1)
     alg = 2 * ms_comp * npts * cs
     achieved = alg / (per_launch_ms / 1e3) / 1e9
-    traffic, fp64_flops = profile_figures(w["name"], precision, KCLASS[dom])
+    traffic, fp64_pct = profile_figures(w["name"], precision, KCLASS[dom])
     r = {"bound": "hbm", "kernel": KCLASS[dom], "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
          "unit": "GB/s", "frac": achieved / peak, "traffic": traffic, "alg_bytes_per_launch": alg,
          "ms_per_launch": per_launch_ms}
-    if fp64_flops and fp64_peak:
-        tf = fp64_flops / (per_launch_ms / 1e3) / 1e12
-        r["fp64"] = {"achieved": tf, "peak": fp64_peak, "unit": "TFLOP/s", "frac": tf / fp64_peak,
-                     "flops_per_launch": fp64_flops, "peak_kind": "measured (fgpe_fp64_fma_rate, this run)"}
+    if fp64_pct is not None:
+        # compute side: the FP64 pipe's active fraction of its peak (ncu),
+        # with this device's FP64 FMA peak measured in the same run
+        r["fp64"] = {"frac": fp64_pct / 100.0, "basis": "sm__pipe_fp64_cycles_active (ncu capture in profiles/)",
+                     "peak": fp64_peak, "unit": "TFLOP/s", "peak_kind": "measured (fgpe_fp64_fma_rate, this run)"}
+    per_class = {}
+    for i in range(4):
+        if kn[i]:
+            tr, pct = profile_figures(w["name"], precision, KCLASS[i])
+            ms = kms[i] / kn[i]
+            per_class[KCLASS[i]] = {"hbm_frac": alg / (ms / 1e3) / 1e9 / peak, "traffic": tr,
+                                    "fp64_pipe_frac": (pct / 100.0) if pct is not None else None}
+    r["per_kernel"] = per_class
     kernels = {KCLASS[i]: {"launches": int(kn[i]), "ms_per_launch": float(kms[i] / kn[i]),
                            "share": float(kms[i] / kms.sum())} for i in range(4) if kn[i]}
     return r, kernels

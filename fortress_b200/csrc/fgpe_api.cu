@@ -74,7 +74,6 @@ struct fgpe_s {
     bool has_fast_row = false, has_fast_col[3] = {false, false, false};
     int fast_row_grid = 0, fast_col_grid[3] = {0, 0, 0};
     bool col_wide[3] = {false, false, false};   // column pass uses the wide tiles
-    int col_split_grid[3] = {0, 0, 0};          // grid of the one-component wide tiles (0: unused)
     // row pass with one warp per x row (k_row_warp), where a row fits 16 KB
     bool has_warp_row = false, warp_row = false;
     int warp_row_grid = 0;
@@ -210,19 +209,6 @@ template <typename T, int MS, int N> constexpr size_t col_smem_w() {
 }
 template <typename T, int MS, int N> constexpr bool wide_ok() { return col_smem_w<T, MS, N>() <= 113 * 1024; }
 template <typename T, int MS, int N> constexpr int col_th_w() { return fast_threads(MS * col_txw<T>() * N / 8); }
-// Column passes without KE/SOC on wide tiles of one component each
-// (FGPE_COL_SPLIT_M = 1 at build time): a third (spin-1) or a fifth (spin-2)
-// of the tile, so more blocks are resident per SM.
-#ifndef FGPE_COL_SPLIT_M
-#define FGPE_COL_SPLIT_M 0
-#endif
-#ifndef FGPE_COL_NBUF_S
-#define FGPE_COL_NBUF_S FGPE_COL_NBUF_W
-#endif
-template <typename T, int N> constexpr size_t col_smem_s() {
-    return (size_t)FGPE_COL_NBUF_S * cpad(N) * col_txw<T>() * sizeof(cx<T>);
-}
-template <typename T, int N> constexpr int col_th_s() { return fast_threads(col_txw<T>() * N / 8); }
 template <typename T, int MS, int N> constexpr size_t row_smem() {
     return ((size_t)FGPE_ROW_NBUF * MS * row_r(N) * cpad(N) + (FGPE_TW_SMEM ? N : 0)) * sizeof(cx<T>);
 }
@@ -248,22 +234,14 @@ template <typename T, int MS, int N> int setup_fast_row(fgpe_t* h) {
 // Grid of the column kernel for one axis (0: none); *wide tells whether the
 // wide tiles were chosen: they need 128-byte rows of x and at least four
 // waves of tiles, so that their fewer, larger tiles still fill the GPU.
-template <typename T, int MS, int N> int setup_fast_col(fgpe_t* h, int axis, int n_other, bool* wide) {
+template <typename T, int MS, int N> int setup_fast_col(fgpe_t* h, int n_other, bool* wide) {
     *wide = false;
     if constexpr (wide_ok<T, MS, N>()) {
         if (h->p.nx % col_txw<T>() == 0) {
             const int ntw = (h->p.nx / col_txw<T>()) * n_other;
             const int g = grid_for(k_col_fast<T, MS, N, col_txw<T>(), col_th_w<T, MS, N>(), FGPE_COL_NBUF_W>, col_th_w<T, MS, N>(),
                                    col_smem_w<T, MS, N>(), ntw);
-            if (g > 0 && ntw >= 4 * g) {
-                *wide = true;
-                if (FGPE_COL_SPLIT_M) {
-                    h->col_split_grid[axis] =
-                        grid_for(k_col_fast<T, 1, N, col_txw<T>(), col_th_s<T, N>(), FGPE_COL_NBUF_S, 1>,
-                                 col_th_s<T, N>(), col_smem_s<T, N>(), ntw * MS);
-                }
-                return g;
-            }
+            if (g > 0 && ntw >= 4 * g) { *wide = true; return g; }
         }
     }
     if (h->p.nx % col_tx<T>()) return 0;
@@ -329,11 +307,6 @@ template <typename T, int MS, int N> void run_warp_row(fgpe_t* h, const RowArgs&
 template <typename T, int MS, int N> void run_fast_col(fgpe_t* h, int axis, const ColArgs& a) {
     if constexpr (wide_ok<T, MS, N>()) {
         if (h->col_wide[axis]) {
-            if (h->col_split_grid[axis] > 0 && !(a.flags & COL_KOP)) {
-                launch_pdl(h, k_col_fast<T, 1, N, col_txw<T>(), col_th_s<T, N>(), FGPE_COL_NBUF_S, 1>,
-                           h->col_split_grid[axis], col_th_s<T, N>(), col_smem_s<T, N>(), a);
-                return;
-            }
             launch_pdl(h, k_col_fast<T, MS, N, col_txw<T>(), col_th_w<T, MS, N>(), FGPE_COL_NBUF_W>, h->fast_col_grid[axis],
                        col_th_w<T, MS, N>(), col_smem_w<T, MS, N>(), a);
             return;
@@ -916,8 +889,8 @@ int fgpe_create(const fgpe_params* pin, fgpe_t** out) {
         const int nob = p.dim == 2 ? 1 : (a == 1 ? p.nz : p.ny);
         int g = 0;
         bool wide = false;
-#define SETC(NN) g = h->fp32 ? (ms == 3 ? setup_fast_col<float, 3, NN>(h, a, nob, &wide) : setup_fast_col<float, 5, NN>(h, a, nob, &wide)) \
-                             : (ms == 3 ? setup_fast_col<double, 3, NN>(h, a, nob, &wide) : setup_fast_col<double, 5, NN>(h, a, nob, &wide))
+#define SETC(NN) g = h->fp32 ? (ms == 3 ? setup_fast_col<float, 3, NN>(h, nob, &wide) : setup_fast_col<float, 5, NN>(h, nob, &wide)) \
+                             : (ms == 3 ? setup_fast_col<double, 3, NN>(h, nob, &wide) : setup_fast_col<double, 5, NN>(h, nob, &wide))
         FAST_SWITCH(ns[a], SETC)
 #undef SETC
         if (g > 0) { h->fast_col[a] = h->has_fast_col[a] = true; h->fast_col_grid[a] = g; h->col_wide[a] = wide; }

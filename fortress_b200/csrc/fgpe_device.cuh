@@ -313,6 +313,18 @@ template <> struct A0<5> {
 // omitted term is below (1/16)^11/11! ~ 8e-22, under FP64 rounding.
 template <typename T> __device__ __forceinline__ cx<T> small_phase(int imag, T th) {
     const T t2 = th * th;
+    if constexpr (sizeof(T) == 4) {
+        // FP32: terms to th^5; the first omitted one is below
+        // (1/16)^6/6! ~ 8e-11, under FP32 rounding (6e-8)
+        if (imag) {
+            const T e = (T)1 - th * ((T)1 - th * ((T)(1.0 / 2) - th * ((T)(1.0 / 6) - th * ((T)(1.0 / 24)
+                        - th * (T)(1.0 / 120)))));
+            return mk<T>(e, (T)0);
+        }
+        const T cs = (T)1 - t2 * ((T)(1.0 / 2) - t2 * (T)(1.0 / 24));
+        const T sn = th * ((T)1 - t2 * ((T)(1.0 / 6) - t2 * (T)(1.0 / 120)));
+        return mk<T>(cs, -sn);
+    }
     if (imag) {
         // exp(-th) = sum (-th)^k/k!
         const T e = (T)1 - th * ((T)1 - th * ((T)(1.0 / 2) - th * ((T)(1.0 / 6) - th * ((T)(1.0 / 24) - th * ((T)(1.0 / 120)
@@ -551,10 +563,17 @@ __device__ __forceinline__ void se_spin1(const StepConst& c, cx<T>* v) {
         // |OMEGA| -> 0 limits (DELTA*CDT^2 = CDT^2/2, KAPPA*CDT = -i CDT) are
         // the leading terms
         const T zz = c.imag ? z : -z;
-        const T g = (T)(1.0 / 2) + zz * ((T)(1.0 / 24) + zz * ((T)(1.0 / 720) + zz * ((T)(1.0 / 40320) +
-                    zz * ((T)(1.0 / 3628800) + zz * (T)(1.0 / 479001600)))));
-        const T f = (T)1 + zz * ((T)(1.0 / 6) + zz * ((T)(1.0 / 120) + zz * ((T)(1.0 / 5040) +
-                    zz * ((T)(1.0 / 362880) + zz * (T)(1.0 / 39916800)))));
+        T g, f;
+        if constexpr (sizeof(T) == 4) {
+            // FP32: to x^4; the next terms are below (1/256)^3/8! ~ 1.5e-12
+            g = (T)(1.0 / 2) + zz * ((T)(1.0 / 24) + zz * (T)(1.0 / 720));
+            f = (T)1 + zz * ((T)(1.0 / 6) + zz * (T)(1.0 / 120));
+        } else {
+            g = (T)(1.0 / 2) + zz * ((T)(1.0 / 24) + zz * ((T)(1.0 / 720) + zz * ((T)(1.0 / 40320) +
+                zz * ((T)(1.0 / 3628800) + zz * (T)(1.0 / 479001600)))));
+            f = (T)1 + zz * ((T)(1.0 / 6) + zz * ((T)(1.0 / 120) + zz * ((T)(1.0 / 5040) +
+                zz * ((T)(1.0 / 362880) + zz * (T)(1.0 / 39916800)))));
+        }
         dc = (c.imag ? (T)1 : (T)-1) * dt * dt * g;
         kc = c.imag ? mk<T>(-dt * f, 0) : mk<T>(0, -dt * f);
     } else {

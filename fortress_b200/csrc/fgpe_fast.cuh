@@ -394,10 +394,7 @@ __global__ void __launch_bounds__(WPB * 32, 2) k_row_warp(StepConst c, RowArgs a
 // --------------------------------------------------------- column kernel
 // Tiles of TX adjacent x positions, full lines of N along the transformed
 // axis; persistent over (x-tile, other) pairs.
-// SPLITM = 1 (with MS = 1): a tile holds one component, its index the
-// slowest part of the tile index; only for passes without KE/SOC, whose
-// components are independent.
-template <typename T, int MS, int N, int TX, int TH, int NBUF = FGPE_COL_NBUF, int SPLITM = 0>
+template <typename T, int MS, int N, int TX, int TH, int NBUF = FGPE_COL_NBUF>
 __global__ void __launch_bounds__(TH, FGPE_COL_MINB) k_col_fast(StepConst c, ColArgs a) {
     asm volatile("griddepcontrol.wait;\n" ::: "memory");
     using CT = ColTile<N, TX>;
@@ -415,8 +412,7 @@ __global__ void __launch_bounds__(TH, FGPE_COL_MINB) k_col_fast(StepConst c, Col
     const long long np = c.npts;
     const int nxt = c.nx / TX;
     const int nother = (int)a.n_other;
-    const int per_m = nxt * nother;
-    const int ntiles = per_m * (SPLITM ? c.ms : 1);
+    const int ntiles = nxt * nother;
     const cx<T>* tw = (const cx<T>*)a.tw;
     if (FGPE_TW_SMEM) {
         cx<T>* tws = bufs + NBUF * TILE;
@@ -427,15 +423,10 @@ __global__ void __launch_bounds__(TH, FGPE_COL_MINB) k_col_fast(StepConst c, Col
     T fac[MS];
 #pragma unroll
     for (int m = 0; m < MS; ++m) fac[m] = (a.flags & COL_SCALE) ? (T)(a.info[INFO_SC + m] * a.cfac) : (T)1;
-    // offset of a tile's first element (its component plane included)
-    auto tile_off = [&](int tile) -> long long {
-        const int mm = SPLITM ? tile / per_m : 0;
-        const int rest = tile - mm * per_m;
-        return (long long)mm * np + (long long)(rest / nxt) * a.other_stride + (rest % nxt) * TX;
-    };
 
     auto issue = [&](int tile, cx<T>* dst) {
-        const long long off = tile_off(tile);
+        const int x0 = (tile % nxt) * TX;
+        const long long off = (long long)(tile / nxt) * a.other_stride + x0;
         for (int ch = threadIdx.x; ch < NCH; ch += TH) {
             const int tc = (ch % CPL) * EPC;
             const int q = ch / CPL;
@@ -462,10 +453,9 @@ __global__ void __launch_bounds__(TH, FGPE_COL_MINB) k_col_fast(StepConst c, Col
             cp_wait<0>();
         }
         __syncthreads();
-        const int x0 = ((SPLITM ? tile % per_m : tile) % nxt) * TX;
-        const int oth = (SPLITM ? tile % per_m : tile) / nxt;
-        const long long off = tile_off(tile);
-        if (SPLITM && (a.flags & COL_SCALE)) fac[0] = (T)(a.info[INFO_SC + tile / per_m] * a.cfac);
+        const int x0 = (tile % nxt) * TX;
+        const int oth = tile / nxt;
+        const long long off = (long long)oth * a.other_stride + x0;
         // with KE/SOC in this pass the scale rides on the pointwise step
         // (the transform is linear); otherwise it takes its own sweep
         const bool fold = (a.flags & COL_SCALE) && (a.flags & COL_KOP);
@@ -482,7 +472,6 @@ __global__ void __launch_bounds__(TH, FGPE_COL_MINB) k_col_fast(StepConst c, Col
             __syncthreads();
         }
         if (a.flags & COL_FWD) ct_fft<T, false, N, MS * TX, TH, CT>(cur, tw);
-        if constexpr (!SPLITM) {
         if (a.flags & COL_KOP) {
             // z lines: (kx, ky) is fixed along each line of the tile, so the
             // SO-coupling exponential is one MS x MS matrix per tile column,
@@ -548,7 +537,6 @@ __global__ void __launch_bounds__(TH, FGPE_COL_MINB) k_col_fast(StepConst c, Col
                 for (int m = 0; m < MS; ++m) cur[(m * LPN + e + (e >> 3)) * TX + t] = v[m];
             }
             __syncthreads();
-        }
         }
         if (a.flags & COL_INV) ct_fft<T, true, N, MS * TX, TH, CT>(cur, tw);
         for (int idx = threadIdx.x; idx < MS * N * TX; idx += TH) {
