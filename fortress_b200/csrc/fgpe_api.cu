@@ -22,6 +22,7 @@
 #include "fgpe_fast.cuh"
 #include "fgpe_group.cuh"
 #include "fno_kernels.cuh"
+#include "fno_gemm_tc.cuh"
 #include "../../include/fno.h"
 
 using namespace fgpe;
@@ -2038,6 +2039,69 @@ int fno_gemm(int batch, int M, int N, int K, float alpha, const void* A, int a_b
         fno::k_gemm<float><<<grid, 256, 0, st>>>(M, N, K, alpha, (const float*)A, sAb, sAi, sAk, B, sBb, sBk, sBj, beta, C,
                                                  sCb, sCi, sCj);
     return fno_ck(cudaGetLastError());
+}
+
+}  // extern "C"
+
+// Tensor-core variant of fno_gemm (fno_gemm_tc.cuh).  When A is shared by
+// every batch entry and B is not, the product is taken transposed (C^T =
+// B^T A^T) so that the shared operand becomes B and the entries fold into one
+// tall GEMM; the tile width GN is the smallest of 16..256 that covers N.
+// CTAs per SM: as many as the shared memory (about 227 KB) and the 512 TMEM
+// columns hold, at most four; CTAs beyond those resident wait their turn.
+template <int GN> constexpr int gemm_tc_per_sm() {
+    const int by_smem = (int)((227 * 1024) / (fno::gtc::smem_bytes<GN>() + 3 * 1024));
+    const int by_tmem = 512 / fno::gtc::tmem_cols<GN>();
+    return std::min(4, std::min(by_smem, by_tmem));
+}
+
+template <typename TA, int GN> static int gemm_tc_launch(const fno::GemmTc& g, cudaStream_t st) {
+    static bool attr_set[64] = {false};
+    int dev = 0, nsm = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return FGPE_E_ARG;
+    const size_t smem = fno::gtc::smem_bytes<GN>();
+    if (!attr_set[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(fno::k_gemm_tc<TA, GN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return fno_ck(e);
+        attr_set[dev] = true;
+    }
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const long long rows = g.fold ? (long long)g.batch * g.M : (long long)g.M;
+    const long long tiles = (rows + fno::gtc::TM - 1) / fno::gtc::TM * ((g.N + GN - 1) / GN) * (g.fold ? 1 : g.batch);
+    const long long grid = std::min<long long>(tiles, (long long)gemm_tc_per_sm<GN>() * nsm);
+    fno::k_gemm_tc<TA, GN><<<(unsigned)grid, 128, smem, st>>>(g);
+    return fno_ck(cudaGetLastError());
+}
+
+template <typename TA> static int gemm_tc_width(const fno::GemmTc& g, cudaStream_t st) {
+    if (g.N <= 16) return gemm_tc_launch<TA, 16>(g, st);
+    if (g.N <= 32) return gemm_tc_launch<TA, 32>(g, st);
+    if (g.N <= 64) return gemm_tc_launch<TA, 64>(g, st);
+    if (g.N <= 128) return gemm_tc_launch<TA, 128>(g, st);
+    return gemm_tc_launch<TA, 256>(g, st);
+}
+
+extern "C" {
+
+int fno_gemm_tc(int batch, int M, int N, int K, float alpha, const void* A, int a_bf16, long long sAb, long long sAi,
+                long long sAk, const float* B, long long sBb, long long sBk, long long sBj, float beta, float* C,
+                long long sCb, long long sCi, long long sCj, int* err_dev, void* stream) {
+    if (!A || !B || !C || !err_dev) { g_last_error = "null argument"; return FGPE_E_ARG; }
+    if (batch <= 0 || M <= 0 || N <= 0 || K <= 0) { g_last_error = "empty GEMM"; return FGPE_E_ARG; }
+    if (sAb < 0 || sAi < 0 || sAk < 0 || sBb < 0 || sBk < 0 || sBj < 0 || sCb < 0 || sCi < 0 || sCj < 0) {
+        g_last_error = "negative stride";
+        return FGPE_E_ARG;
+    }
+    fno::GemmTc g{M, N, K, batch, 0, alpha, beta, A, sAb, sAi, sAk, B, sBb, sBk, sBj, C, sCb, sCi, sCj, err_dev};
+    if (batch > 1 && sAb == 0 && sBb != 0 && !a_bf16) {
+        // C^T = B^T A^T: the shared A becomes the B operand
+        g = fno::GemmTc{N, M, K, batch, 0, alpha, beta, B, sBb, sBj, sBk, (const float*)A, 0, sAk, sAi,
+                        C, sCb, sCj, sCi, err_dev};
+    }
+    g.fold = batch > 1 && g.sBb == 0;
+    const cudaStream_t st = (cudaStream_t)stream;
+    return a_bf16 ? gemm_tc_width<__nv_bfloat16>(g, st) : gemm_tc_width<float>(g, st);
 }
 
 int fno_bias_act(float* z, float* h, const float* bias, long long C, long long S, long long n, int act, void* stream) {

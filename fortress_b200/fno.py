@@ -16,10 +16,14 @@ Layout on the device: channel-major activations [C][B][N][N] (float32), so a
 pointwise channel mix is one GEMM over all B*N*N points; those dense layers
 (and their input gradients) run on the tensor cores (fno_dense_tc: tcgen05,
 BF16 operands, FP32 accumulation in tensor memory, bias and GELU fused).
-Weights keep an FP32 master copy (Adam) and a BF16 copy that the GEMMs read.  The spectral convolution is five GEMM stages over real/imaginary
-planes (truncated DFTs as dense matrices), the per-mode channel mix a batched
-GEMM over the 2*NM*NM retained modes in the real block form
-[[Rr, -Ri], [Ri, Rr]].
+Weights keep an FP32 master copy (Adam) and a BF16 copy that the GEMMs read.
+The spectral convolution is five GEMM stages over real/imaginary planes
+(truncated DFTs as dense matrices), the per-mode channel mix a batched GEMM
+over the 2*NM*NM retained modes in the real block form [[Rr, -Ri], [Ri, Rr]].
+With tensor_cores (the default) these stages and their backward and
+weight-gradient products run on fno_gemm_tc: tcgen05 with each FP32 operand
+split into a BF16 head and tail (about 16 significant bits), FP32
+accumulation in tensor memory.
 
 Device memory comes from torch (plumbing only); every arithmetic step is a
 kernel of libfgpe.so.
@@ -33,7 +37,7 @@ import numpy as np
 from . import _abi
 
 FNO_EXPORTS = ("fno_gemm", "fno_bias_act", "fno_act_bwd", "fno_channel_sum", "fno_axpy", "fno_mse",
-               "fno_adam", "fno_to_bf16", "fno_rbig_build", "fno_rbig_fold", "fno_dense_tc")
+               "fno_adam", "fno_to_bf16", "fno_rbig_build", "fno_rbig_fold", "fno_dense_tc", "fno_gemm_tc")
 
 _L = None
 
@@ -56,6 +60,7 @@ def lib():
         "fno_rbig_build": [vp, vp, vp, ll, ip, ip, vp],
         "fno_rbig_fold": [vp, vp, vp, ll, ip, ip, vp],
         "fno_dense_tc": [vp, ip, vp, vp, vp, vp, ip, ip, ll, ip, vp, vp],
+        "fno_gemm_tc": [ip, ip, ip, ip, fl, vp, ip, ll, ll, ll, vp, ll, ll, ll, fl, vp, ll, ll, ll, vp, vp],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -104,7 +109,8 @@ class FNO:
         import torch
         self.torch = torch
         # dense (pointwise) layers on tcgen05 (BF16 operands, FP32 accumulation)
-        # when their channel counts fit one 128-row tile; else the FP32 GEMM
+        # when their channel counts fit one 128-row tile, and the spectral
+        # stages on the split-BF16 tcgen05 GEMM (fno_gemm_tc); else the FP32 GEMM
         self.tensor_cores = tensor_cores
         self.tc_err = torch.zeros(1, dtype=torch.int32, device=device)
         self.L = lib()
@@ -239,10 +245,13 @@ class FNO:
 
     def gemm(self, batch, M, N, K, A, sA, B_, sB, C, sC, alpha=1.0, beta=0.0, a_bf16=False, aoff=0, boff=0, coff=0):
         ea = 2 if a_bf16 else 4
-        rc = self.L.fno_gemm(batch, M, N, K, alpha, ctypes.c_void_p(A.data_ptr() + ea * aoff), int(a_bf16),
-                             sA[0], sA[1], sA[2], ctypes.c_void_p(B_.data_ptr() + 4 * boff), sB[0], sB[1], sB[2],
-                             beta, ctypes.c_void_p(C.data_ptr() + 4 * coff), sC[0], sC[1], sC[2], self._st())
-        _ck(rc, "gemm")
+        args = (batch, M, N, K, alpha, ctypes.c_void_p(A.data_ptr() + ea * aoff), int(a_bf16),
+                sA[0], sA[1], sA[2], ctypes.c_void_p(B_.data_ptr() + 4 * boff), sB[0], sB[1], sB[2],
+                beta, ctypes.c_void_p(C.data_ptr() + 4 * coff), sC[0], sC[1], sC[2])
+        if self.tensor_cores:
+            _ck(self.L.fno_gemm_tc(*args, self._p(self.tc_err), self._st()), "gemm_tc")
+        else:
+            _ck(self.L.fno_gemm(*args, self._st()), "gemm")
 
     def _use_tc(self, M, K):
         return self.tensor_cores and M <= 128 and K <= 128

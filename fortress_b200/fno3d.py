@@ -23,6 +23,8 @@ truncated DFT along x, then y, then z (three batched GEMM stages over
 real/imaginary planes), a per-mode channel mix (batched GEMM over the F*F*M
 modes in the real block form [[Rr, -Ri], [Ri, Rr]]), and the inverse stages
 in reverse order; the backward pass runs the transposed stages by strides.
+With tensor_cores (the default) those stages run on fno_gemm_tc (tcgen05,
+FP32 operands split into BF16 head and tail, FP32 accumulation).
 Device memory comes from torch (plumbing only); every arithmetic step is a
 kernel of libfgpe.so.
 """
@@ -229,10 +231,13 @@ class FNO3:
     def gemm(self, batch, M, N, K, A, sA, B_, sB, C, sC, alpha=1.0, beta=0.0, a_bf16=False, aoff=0, boff=0, coff=0):
         import ctypes
         ea = 2 if a_bf16 else 4
-        rc = self.L.fno_gemm(batch, M, N, K, alpha, ctypes.c_void_p(A.data_ptr() + ea * aoff), int(a_bf16),
-                             sA[0], sA[1], sA[2], ctypes.c_void_p(B_.data_ptr() + 4 * boff), sB[0], sB[1], sB[2],
-                             beta, ctypes.c_void_p(C.data_ptr() + 4 * coff), sC[0], sC[1], sC[2], self._st())
-        _ck(rc, "gemm")
+        args = (batch, M, N, K, alpha, ctypes.c_void_p(A.data_ptr() + ea * aoff), int(a_bf16),
+                sA[0], sA[1], sA[2], ctypes.c_void_p(B_.data_ptr() + 4 * boff), sB[0], sB[1], sB[2],
+                beta, ctypes.c_void_p(C.data_ptr() + 4 * coff), sC[0], sC[1], sC[2])
+        if self.tensor_cores:
+            _ck(self.L.fno_gemm_tc(*args, self._p(self.tc_err), self._st()), "gemm_tc")
+        else:
+            _ck(self.L.fno_gemm(*args, self._st()), "gemm")
 
     def _use_tc(self, M, K):
         return self.tensor_cores and M <= 128 and K <= 128

@@ -21,6 +21,16 @@ extern "C" {
 int fno_gemm(int batch, int M, int N, int K, float alpha, const void *A, int a_bf16, long long sAb,
              long long sAi, long long sAk, const float *B, long long sBb, long long sBk, long long sBj,
              float beta, float *C, long long sCb, long long sCi, long long sCj, void *stream);
+/* fno_gemm on the tensor cores (tcgen05.mma, FP32 accumulation in tensor
+ * memory): each FP32 operand is split into a bfloat16 head and tail and the
+ * product keeps hi*hi + hi*lo + lo*hi (about 16 significant bits per
+ * operand; a bfloat16 A is exact).  Strides must be >= 0.  When B is shared
+ * by all batch entries (sBb == 0), or A is (sAb == 0, taken transposed), the
+ * entries' rows form one tall GEMM.  *err_dev (device int) is set to 1 if a
+ * CTA's wait for its accumulator ran out. */
+int fno_gemm_tc(int batch, int M, int N, int K, float alpha, const void *A, int a_bf16, long long sAb,
+                long long sAi, long long sAk, const float *B, long long sBb, long long sBk, long long sBj,
+                float beta, float *C, long long sCb, long long sCi, long long sCj, int *err_dev, void *stream);
 /* z[b,c,s] += bias[c] (bias may be NULL); h = GELU(z) if act else z (h may be NULL). */
 int fno_bias_act(float *z, float *h, const float *bias, long long C, long long S, long long n, int act, void *stream);
 /* dz = dh * GELU'(z) */

@@ -86,3 +86,16 @@ def test_argument_errors_need_no_device():
         F.Propagator(dim=2, spin=1, n=(32, 14), d=(0.1, 0.1), dt=1e-3, imag_time=1, tau=(1.0, 0.0, 0.0))
     with pytest.raises(F.FgpeError):
         F.Propagator(dim=1, spin=1, n=(32,), d=(0.1,), dt=-1.0, imag_time=1, tau=(1.0, 0.0, 0.0))
+
+
+def test_fno_gemm_tc_argument_errors_need_no_device():
+    from fortress_b200 import fno
+    L = fno.lib()
+    p = ctypes.c_void_p(16)            # never dereferenced: the checks come first
+    ok = (2, 8, 8, 8, 1.0, p, 0, 64, 8, 1, p, 0, 8, 1, 0.0, p, 64, 8, 1)
+    assert L.fno_gemm_tc(*ok[:5], None, *ok[6:], p, None) == _abi.FGPE_E_ARG       # null A
+    assert L.fno_gemm_tc(*ok, None, None) == _abi.FGPE_E_ARG                       # null error flag
+    assert L.fno_gemm_tc(0, *ok[1:], p, None) == _abi.FGPE_E_ARG                   # empty batch
+    bad = list(ok)
+    bad[12] = -1                                                                   # negative sBb
+    assert L.fno_gemm_tc(*bad, p, None) == _abi.FGPE_E_ARG
