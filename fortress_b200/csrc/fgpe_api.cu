@@ -2093,13 +2093,21 @@ int fno_gemm_tc(int batch, int M, int N, int K, float alpha, const void* A, int 
         g_last_error = "negative stride";
         return FGPE_E_ARG;
     }
-    fno::GemmTc g{M, N, K, batch, 0, alpha, beta, A, sAb, sAi, sAk, B, sBb, sBk, sBj, C, sCb, sCi, sCj, err_dev};
+    fno::GemmTc g{M, N, K, batch, 0, alpha, beta, A, sAb, sAi, sAk, B, sBb, sBk, sBj, C, sCb, sCi, sCj, err_dev, 0, 0, 0};
     if (batch > 1 && sAb == 0 && sBb != 0 && !a_bf16) {
         // C^T = B^T A^T: the shared A becomes the B operand
         g = fno::GemmTc{N, M, K, batch, 0, alpha, beta, B, sBb, sBj, sBk, (const float*)A, 0, sAk, sAi,
-                        C, sCb, sCj, sCi, err_dev};
+                        C, sCb, sCj, sCi, err_dev, 0, 0, 0};
     }
     g.fold = batch > 1 && g.sBb == 0;
+    // float4 operand reads where the unit-stride runs start on 16-byte boundaries
+    const bool a16 = ((uintptr_t)g.A & 15) == 0, b16 = ((uintptr_t)g.B & 15) == 0;
+    g.avec = !a_bf16 && a16 && g.sAk == 1 && g.sAi % 4 == 0 && g.sAb % 4 == 0;
+    if (b16 && g.sBb % 4 == 0) {
+        if (g.sBj == 1 && g.sBk % 4 == 0) g.bvec = 1;
+        else if (g.sBk == 1 && g.sBj % 4 == 0) g.bvec = 2;
+    }
+    g.cvec = ((uintptr_t)g.C & 15) == 0 && g.sCj == 1 && g.sCi % 4 == 0 && g.sCb % 4 == 0;
     const cudaStream_t st = (cudaStream_t)stream;
     return a_bf16 ? gemm_tc_width<__nv_bfloat16>(g, st) : gemm_tc_width<float>(g, st);
 }
@@ -2115,7 +2123,10 @@ int fno_act_bwd(float* dz, const float* dh, const float* z, long long n, void* s
 }
 
 int fno_channel_sum(float* out, const float* x, long long B, long long C, long long S, float beta, void* stream) {
-    fno::k_channel_sum<<<(unsigned)C, 256, 0, (cudaStream_t)stream>>>(out, x, B, C, S, beta);
+    if (S == 1)
+        fno::k_channel_sum_rows<<<(unsigned)((C + 255) / 256), 256, 0, (cudaStream_t)stream>>>(out, x, B, C, beta);
+    else
+        fno::k_channel_sum<<<(unsigned)C, 256, 0, (cudaStream_t)stream>>>(out, x, B, C, S, beta);
     return fno_ck(cudaGetLastError());
 }
 

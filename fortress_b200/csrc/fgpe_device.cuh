@@ -59,6 +59,13 @@ template <typename T> __device__ __forceinline__ cx<T> cdt_phase(int imag, T dt,
     return mk<T>(c, -s);
 }
 
+// a * b where a is an exp(-i CDT x) factor: in imaginary time (CDT = -i DT)
+// a is real, so the product is a scale (2 multiplies instead of 4 and 2 adds)
+template <typename C> __device__ __forceinline__ C fmul(int imag, C a, C b) {
+    if (imag) { b.x *= a.x; b.y *= a.x; return b; }
+    return cmul(a, b);
+}
+
 // ------------------------------------------------------------------- FFT
 // A transform length n = prod(r[0..nf-1]), radices from {2,3,4,5,8}.
 //
@@ -419,14 +426,14 @@ template <typename T, int MS>
 __device__ __forceinline__ void apply_ke(const StepConst& c, int ix, int iy, int iz, cx<T>* v) {
     const cx<T>* kex = (const cx<T>*)c.kex;
     cx<T> f = kex[ix];
-    if (c.dim >= 2) f = cmul(f, ((const cx<T>*)c.key)[iy]);
+    if (c.dim >= 2) f = fmul(c.imag, f, ((const cx<T>*)c.key)[iy]);
     if (c.dim == 3) {
         const cx<T>* kez = (const cx<T>*)c.kez;
 #pragma unroll
-        for (int m = 0; m < MS; ++m) v[m] = cmul(v[m], cmul(f, kez[m * c.nz + iz]));
+        for (int m = 0; m < MS; ++m) v[m] = fmul(c.imag, fmul(c.imag, f, kez[m * c.nz + iz]), v[m]);
     } else {
 #pragma unroll
-        for (int m = 0; m < MS; ++m) v[m] = cmul(v[m], f);
+        for (int m = 0; m < MS; ++m) v[m] = fmul(c.imag, f, v[m]);
     }
 }
 
@@ -554,7 +561,7 @@ __device__ __forceinline__ void se_spin1(const StepConst& c, cx<T>* v) {
     const T r2 = aa + bb;
     const T dt = (T)c.dt;
     T dc;                 // DELTA*CDT^2 (real)
-    cx<T> kc;             // KAPPA*CDT
+    T kf;                 // KAPPA*CDT = kf (imaginary time) or i kf (real time)
     const T z = dt * dt * r2;   // |OMEGA|^2
     if (z <= (T)(1.0 / 256)) {
         // |OMEGA| <= 1/16: 2 sinh^2(x/2)/x^2 = sum x^2n/(2n+2)!, sinh(x)/x =
@@ -575,26 +582,28 @@ __device__ __forceinline__ void se_spin1(const StepConst& c, cx<T>* v) {
                 zz * ((T)(1.0 / 362880) + zz * (T)(1.0 / 39916800)))));
         }
         dc = (c.imag ? (T)1 : (T)-1) * dt * dt * g;
-        kc = c.imag ? mk<T>(-dt * f, 0) : mk<T>(0, -dt * f);
+        kf = -dt * f;
     } else {
     const T r = sqrt_t(r2);
     const T x = dt * r;   // |OMEGA|
     const bool big = c.se_ge ? (x >= (T)1e-40) : (x > (T)1e-40);
     if (c.imag) {
-        if (big) { T sh = sinh_t((T)0.5 * x); dc = (T)2 * sh * sh / r2; kc = mk<T>(-sinh_t(x) / r, 0); }
-        else { dc = (T)0.5 * dt * dt; kc = mk<T>(-dt, 0); }
+        if (big) { T sh = sinh_t((T)0.5 * x); dc = (T)2 * sh * sh / r2; kf = -sinh_t(x) / r; }
+        else { dc = (T)0.5 * dt * dt; kf = -dt; }
     } else {
-        if (big) { T sn = sin_t((T)0.5 * x); dc = (T)-2 * sn * sn / r2; kc = mk<T>(0, -sin_t(x) / r); }
-        else { dc = (T)-0.5 * dt * dt; kc = mk<T>(0, -dt); }
+        if (big) { T sn = sin_t((T)0.5 * x); dc = (T)-2 * sn * sn / r2; kf = -sin_t(x) / r; }
+        else { dc = (T)-0.5 * dt * dt; kf = -dt; }
     }
     }
     const cx<T> p1 = v[0], p2 = v[1], p3 = v[2];
-    // TMP(1) = dc (|A1|^2 p1 + A1 B1* p3) + kc A1 p2
+    // TMP(1) = dc (|A1|^2 p1 + A1 B1* p3) + KAPPA*CDT A1 p2
     cx<T> u1 = cadd(cscale(p1, aa), cmul(cmulc(A1, B1), p3));
     cx<T> u3 = cadd(cmul(cmulc(B1, A1), p1), cscale(p3, bb));
-    cx<T> w1 = cmul(kc, cmul(A1, p2));
-    cx<T> w2 = cmul(kc, cadd(cmulc(p1, A1), cmulc(p3, B1)));
-    cx<T> w3 = cmul(kc, cmul(B1, p2));
+    // KAPPA*CDT is real or purely imaginary: its products are two multiplies
+    auto kmul = [&](cx<T> q) { return c.imag ? mk<T>(kf * q.x, kf * q.y) : mk<T>(-kf * q.y, kf * q.x); };
+    cx<T> w1 = kmul(cmul(A1, p2));
+    cx<T> w2 = kmul(cadd(cmulc(p1, A1), cmulc(p3, B1)));
+    cx<T> w3 = kmul(cmul(B1, p2));
     v[0] = cadd(p1, cadd(cscale(u1, dc), w1));
     v[1] = cadd(p2, cadd(cscale(p2, dc * r2), w2));
     v[2] = cadd(p3, cadd(cscale(u3, dc), w3));
@@ -606,8 +615,8 @@ __device__ __forceinline__ void se_spin1(const StepConst& c, cx<T>* v) {
 template <typename T>
 __device__ __forceinline__ cx<T> pot_phase(const StepConst& c, int i, int j, int k) {
     cx<T> e = ((const cx<T>*)c.pvx)[i];
-    if (c.dim >= 2) e = cmul(e, ((const cx<T>*)c.pvy)[j]);
-    if (c.dim >= 3) e = cmul(e, ((const cx<T>*)c.pvz)[k]);
+    if (c.dim >= 2) e = fmul(c.imag, e, ((const cx<T>*)c.pvy)[j]);
+    if (c.dim >= 3) e = fmul(c.imag, e, ((const cx<T>*)c.pvz)[k]);
     return e;
 }
 
@@ -634,14 +643,17 @@ __device__ __forceinline__ void apply_sp(const StepConst& c, cx<T> eV, cx<T>* v)
         B[MS - 2] = -t1 * fz + (T)0.4 * t2 * a[1];
         B[MS - 1] = (T)-2 * t1 * fz + (T)0.4 * t2 * a[0];
     }
+    // one phase per component for the density parts, exp(-i CDT (tau0 rho +
+    // B_m)), as the reference takes one exponential of T_m (cgpe1d.f90:
+    // 871-873, 890-892); in imaginary time every factor is real
     const T dt = (T)c.dt;
-    const T th0 = dt * t0 * rho;
-    const cx<T> eA = cmul(eV, fabs(th0) <= (T)0.0625 ? small_phase<T>(c.imag, th0) : cdt_phase<T>(c.imag, dt, t0 * rho));
+    const T d0 = t0 * rho;
 #pragma unroll
     for (int m = 0; m < MS; ++m) {
-        const T th = dt * B[m];
-        const cx<T> eB = fabs(th) <= (T)0.0625 ? small_phase<T>(c.imag, th) : cdt_phase<T>(c.imag, dt, B[m]);
-        v[m] = cmul(v[m], cmul(eA, eB));
+        const T x = d0 + B[m];
+        const T th = dt * x;
+        const cx<T> eB = fabs(th) <= (T)0.0625 ? small_phase<T>(c.imag, th) : cdt_phase<T>(c.imag, dt, x);
+        v[m] = fmul(c.imag, fmul(c.imag, eV, eB), v[m]);
     }
 }
 

@@ -488,7 +488,7 @@ __global__ void __launch_bounds__(TH, FGPE_COL_MINB) k_col_fast(StepConst c, Col
                     apply_soc<T, MS>(c, c.kx[ixt], c.ky[iyt], u);
                     // the kx, ky part of KE, exp(-i CDT (kx^2 + ky^2)), is a
                     // scalar along the line: folded into the matrix
-                    const cx<T> f = (a.flags & COL_KE) ? cmul(((const cx<T>*)c.kex)[ixt], ((const cx<T>*)c.key)[iyt])
+                    const cx<T> f = (a.flags & COL_KE) ? fmul(c.imag, ((const cx<T>*)c.kex)[ixt], ((const cx<T>*)c.key)[iyt])
                                                         : mk<T>((T)1, (T)0);
 #pragma unroll
                     for (int r = 0; r < MS; ++r) usoc[(t * MS + r) * MS + j] = cmul(u[r], f);
@@ -513,7 +513,7 @@ __global__ void __launch_bounds__(TH, FGPE_COL_MINB) k_col_fast(StepConst c, Col
                         // the kz part, exp(-i CDT (kz^2 - 2 L GAMMAZ kz)) per component
                         const cx<T>* kez = (const cx<T>*)c.kez;
 #pragma unroll
-                        for (int m = 0; m < MS; ++m) v[m] = cmul(v[m], kez[m * c.nz + iz]);
+                        for (int m = 0; m < MS; ++m) v[m] = fmul(c.imag, kez[m * c.nz + iz], v[m]);
                     }
                 } else if (a.flags & COL_KE) {
                     apply_ke<T, MS>(c, ix, iy, iz, v);

@@ -44,6 +44,9 @@ struct GemmTc {
     float* C;
     long long sCb, sCi, sCj;
     int* err;
+    int avec;           // 1: FP32 A read as float4 along K (contiguous, 16-byte aligned rows)
+    int bvec;           // 1: B read as float4 along N; 2: along K (likewise)
+    int cvec;           // 1: C rows contiguous along N on 16-byte boundaries (float4 epilogue)
 };
 
 namespace gtc {
@@ -90,6 +93,17 @@ __device__ __forceinline__ float ld_any(const __nv_bfloat16* p) { return __bfloa
 __device__ __forceinline__ void split_bf16(float v, __nv_bfloat16& hi, __nv_bfloat16& lo) {
     hi = __float2bfloat16_rn(v);
     lo = __float2bfloat16_rn(v - __bfloat162float(hi));
+}
+
+// four consecutive elements of one core-matrix row (8 bytes): head and tail
+__device__ __forceinline__ void put4(unsigned char* h, unsigned char* l, int off, float4 v) {
+    __nv_bfloat16 hi[4], lo[4];
+    split_bf16(v.x, hi[0], lo[0]);
+    split_bf16(v.y, hi[1], lo[1]);
+    split_bf16(v.z, hi[2], lo[2]);
+    split_bf16(v.w, hi[3], lo[3]);
+    *(uint2*)(h + off) = *(const uint2*)hi;
+    *(uint2*)(l + off) = *(const uint2*)lo;
 }
 
 __device__ __forceinline__ void mma(uint32_t tmem, uint64_t da, uint64_t db, uint32_t id, uint32_t acc) {
@@ -171,58 +185,145 @@ __global__ void __launch_bounds__(128, 1) k_gemm_tc(GemmTc g) {
         const long long bofs = g.fold ? 0 : bq * g.sBb;
         __syncthreads();
         for (int k0 = 0; k0 < g.K && ok; k0 += KC) {
-            // A slice, walking the contiguous index fastest across threads;
-            // each thread issues LB independent loads before it converts and
-            // stores them (the loads' latency overlaps)
-            const bool akf = g.sAk == 1;
+            // K extent staged this round, a multiple of 16 (the products read
+            // no further): short K (the retained modes) stages only its columns
+            const int kx = min(KC, (g.K - k0 + 15) / 16 * 16);
+            const int kx4 = kx / 4;
+            if (A_SPLIT && g.avec) {
+                // A rows as float4 along K: 16 consecutive threads read one
+                // row's 256-byte slice; 8 vectors in flight per thread
 #pragma unroll 1
-            for (int e0 = 0; e0 < TM * KC; e0 += 128 * LB) {
-                float v[LB];
+                for (int e0 = 0; e0 < TM * kx4; e0 += 128 * 8) {
+                    float4 v[8];
 #pragma unroll
-                for (int j = 0; j < LB; ++j) {
-                    const int e = e0 + tid + j * 128;
-                    const int m = akf ? e / KC : e % TM, k = akf ? e % KC : e / TM;
-                    const long long oa = rowA[m];
-                    v[j] = (oa >= 0 && k0 + k < g.K) ? ld_any(A + oa + (long long)(k0 + k) * g.sAk) : 0.f;
+                    for (int j = 0; j < 8; ++j) {
+                        const int e = min(e0 + tid + j * 128, TM * kx4 - 1);
+                        const int m = e / kx4, kq = (e % kx4) * 4;
+                        const long long oa = rowA[m];
+                        const float* src = (const float*)A + oa + k0 + kq;
+                        if (oa >= 0 && k0 + kq + 3 < g.K) {
+                            v[j] = *(const float4*)src;
+                        } else {
+                            v[j].x = (oa >= 0 && k0 + kq < g.K) ? src[0] : 0.f;
+                            v[j].y = (oa >= 0 && k0 + kq + 1 < g.K) ? src[1] : 0.f;
+                            v[j].z = (oa >= 0 && k0 + kq + 2 < g.K) ? src[2] : 0.f;
+                            v[j].w = 0.f;
+                        }
+                    }
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        const int e = e0 + tid + j * 128;
+                        if (e < TM * kx4) {
+                            const int m = e / kx4, kq = (e % kx4) * 4;
+                            put4(sAh, sAl, a_off(m, kq), v[j]);
+                        }
+                    }
                 }
+            } else {
+                // A slice, walking the contiguous index fastest across threads;
+                // each thread issues LB independent loads before it converts and
+                // stores them (the loads' latency overlaps)
+                const bool akf = g.sAk == 1;
+#pragma unroll 1
+                for (int e0 = 0; e0 < TM * kx; e0 += 128 * LB) {
+                    float v[LB];
 #pragma unroll
-                for (int j = 0; j < LB; ++j) {
-                    const int e = e0 + tid + j * 128;
-                    const int m = akf ? e / KC : e % TM, k = akf ? e % KC : e / TM;
-                    const int off = a_off(m, k);
-                    if (A_SPLIT) {
-                        bf16 hi, lo;
-                        split_bf16(v[j], hi, lo);
-                        *(bf16*)(sAh + off) = hi;
-                        *(bf16*)(sAl + off) = lo;
-                    } else {
-                        *(bf16*)(sAh + off) = __float2bfloat16_rn(v[j]);   // exact: v came from BF16
+                    for (int j = 0; j < LB; ++j) {
+                        const int e = min(e0 + tid + j * 128, TM * kx - 1);   // TM*kx is a multiple of 128*LB
+                        const int m = akf ? e / kx : e % TM, k = akf ? e % kx : e / TM;
+                        const long long oa = rowA[m];
+                        v[j] = (oa >= 0 && k0 + k < g.K) ? ld_any(A + oa + (long long)(k0 + k) * g.sAk) : 0.f;
+                    }
+#pragma unroll
+                    for (int j = 0; j < LB; ++j) {
+                        const int e = e0 + tid + j * 128;
+                        if (e >= TM * kx) continue;
+                        const int m = akf ? e / kx : e % TM, k = akf ? e % kx : e / TM;
+                        const int off = a_off(m, k);
+                        if (A_SPLIT) {
+                            bf16 hi, lo;
+                            split_bf16(v[j], hi, lo);
+                            *(bf16*)(sAh + off) = hi;
+                            *(bf16*)(sAl + off) = lo;
+                        } else {
+                            *(bf16*)(sAh + off) = __float2bfloat16_rn(v[j]);   // exact: v came from BF16
+                        }
                     }
                 }
             }
-            // B slice
-            const bool bnf = g.sBj == 1;
+            if (g.bvec) {
+                // B as float4 along N (bvec 1) or along K (bvec 2)
+                const bool nvec = g.bvec == 1;
+                const int NV = kx * GN / 4;
 #pragma unroll 1
-            for (int e0 = 0; e0 < KC * GN; e0 += 128 * LB) {
-                float v[LB];
+                for (int e0 = 0; e0 < NV; e0 += 128 * 8) {
+                    float4 v[8];
 #pragma unroll
-                for (int j = 0; j < LB; ++j) {
-                    const int e = e0 + tid + j * 128;
-                    const int n = bnf ? e % GN : e / KC, k = bnf ? e / GN : e % KC;
-                    v[j] = (e < KC * GN && k0 + k < g.K && n0 + n < g.N)
-                               ? g.B[bofs + (long long)(k0 + k) * g.sBk + (long long)(n0 + n) * g.sBj]
-                               : 0.f;
+                    for (int j = 0; j < 8; ++j) {
+                        const int e = e0 + tid + j * 128;
+                        v[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+                        if (e < NV) {
+                            const int k = nvec ? e / (GN / 4) : (e % kx4) * 4;
+                            const int n = nvec ? (e % (GN / 4)) * 4 : e / kx4;
+                            const float* src = g.B + bofs + (long long)(k0 + k) * g.sBk + (long long)(n0 + n) * g.sBj;
+                            const int lim = nvec ? (k0 + k < g.K ? g.N - (n0 + n) : 0) : (n0 + n < g.N ? g.K - (k0 + k) : 0);
+                            // the vector runs along the unit-stride index
+                            if (lim >= 4) {
+                                v[j] = *(const float4*)src;
+                            } else {
+                                if (lim > 0) v[j].x = src[0];
+                                if (lim > 1) v[j].y = src[1];
+                                if (lim > 2) v[j].z = src[2];
+                            }
+                        }
+                    }
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        const int e = e0 + tid + j * 128;
+                        if (e < NV) {
+                            if (nvec) {
+                                const int k = e / (GN / 4), nq = (e % (GN / 4)) * 4;
+                                put4(sBh, sBl, b_off<GN>(k, nq), v[j]);
+                            } else {
+                                const int kq = (e % kx4) * 4, n = e / kx4;
+                                const float f[4] = {v[j].x, v[j].y, v[j].z, v[j].w};
+#pragma unroll
+                                for (int q = 0; q < 4; ++q) {
+                                    bf16 hi, lo;
+                                    split_bf16(f[q], hi, lo);
+                                    const int off = b_off<GN>(kq + q, n);
+                                    *(bf16*)(sBh + off) = hi;
+                                    *(bf16*)(sBl + off) = lo;
+                                }
+                            }
+                        }
+                    }
                 }
+            } else {
+                // B slice
+                const bool bnf = g.sBj == 1;
+#pragma unroll 1
+                for (int e0 = 0; e0 < kx * GN; e0 += 128 * LB) {
+                    float v[LB];
 #pragma unroll
-                for (int j = 0; j < LB; ++j) {
-                    const int e = e0 + tid + j * 128;
-                    if (e < KC * GN) {
-                        const int n = bnf ? e % GN : e / KC, k = bnf ? e / GN : e % KC;
-                        bf16 hi, lo;
-                        split_bf16(v[j], hi, lo);
-                        const int off = b_off<GN>(k, n);
-                        *(bf16*)(sBh + off) = hi;
-                        *(bf16*)(sBl + off) = lo;
+                    for (int j = 0; j < LB; ++j) {
+                        const int e = e0 + tid + j * 128;
+                        const int n = bnf ? e % GN : e / kx, k = bnf ? e / GN : e % kx;
+                        v[j] = (e < kx * GN && k0 + k < g.K && n0 + n < g.N)
+                                   ? g.B[bofs + (long long)(k0 + k) * g.sBk + (long long)(n0 + n) * g.sBj]
+                                   : 0.f;
+                    }
+#pragma unroll
+                    for (int j = 0; j < LB; ++j) {
+                        const int e = e0 + tid + j * 128;
+                        if (e < kx * GN) {
+                            const int n = bnf ? e % GN : e / kx, k = bnf ? e / GN : e % kx;
+                            bf16 hi, lo;
+                            split_bf16(v[j], hi, lo);
+                            const int off = b_off<GN>(k, n);
+                            *(bf16*)(sBh + off) = hi;
+                            *(bf16*)(sBl + off) = lo;
+                        }
                     }
                 }
             }
@@ -266,14 +367,40 @@ __global__ void __launch_bounds__(128, 1) k_gemm_tc(GemmTc g) {
                 : "r"(taddr));
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
             if (oc >= 0) {
+                const int nb = n0 + cb * 16;
+                float* crow = g.C + oc + (long long)nb * g.sCj;
+                float out[16];
 #pragma unroll
-                for (int j = 0; j < 16; ++j) {
-                    const int n = n0 + cb * 16 + j;
-                    if (n < g.N) {
-                        float* c = g.C + oc + (long long)n * g.sCj;
-                        const float v = g.alpha * __uint_as_float(r[j]);
-                        *c = g.beta == 0.f ? v : v + g.beta * *c;
+                for (int j = 0; j < 16; ++j) out[j] = g.alpha * __uint_as_float(r[j]);
+                if (g.cvec && nb + 16 <= g.N) {
+                    // 64 contiguous bytes of the row: float4 reads and writes
+                    float4* c4 = (float4*)crow;
+                    if (g.beta != 0.f) {
+                        float4 o[4];
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) o[q] = c4[q];
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            out[4 * q] += g.beta * o[q].x;
+                            out[4 * q + 1] += g.beta * o[q].y;
+                            out[4 * q + 2] += g.beta * o[q].z;
+                            out[4 * q + 3] += g.beta * o[q].w;
+                        }
                     }
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) c4[q] = make_float4(out[4 * q], out[4 * q + 1], out[4 * q + 2], out[4 * q + 3]);
+                } else {
+                    // all reads of C before any write, so they overlap
+                    if (g.beta != 0.f) {
+                        float o[16];
+#pragma unroll
+                        for (int j = 0; j < 16; ++j) o[j] = nb + j < g.N ? crow[(long long)j * g.sCj] : 0.f;
+#pragma unroll
+                        for (int j = 0; j < 16; ++j) out[j] += g.beta * o[j];
+                    }
+#pragma unroll
+                    for (int j = 0; j < 16; ++j)
+                        if (nb + j < g.N) crow[(long long)j * g.sCj] = out[j];
                 }
             }
         }

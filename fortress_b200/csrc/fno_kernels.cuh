@@ -100,12 +100,34 @@ __global__ void k_act_bwd(float* dz, const float* dh, const float* z, long long 
         dz[t] = dh[t] * gelu_g(z[t]);
 }
 
-// out[c] = beta*out[c] + sum_{b,s} x[b,c,s]; one block per channel, fixed order.
+// out[c] = beta*out[c] + sum_{b,s} x[b,c,s] in a fixed order.  S == 1 (the
+// per-chunk weight-gradient partials): one thread per channel walks b, the
+// reads coalesced across channels.  Otherwise one block per channel, each
+// thread with eight independent accumulators over its strided elements.
+__global__ void k_channel_sum_rows(float* out, const float* x, long long B, long long C, float beta) {
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= C) return;
+    double acc = 0.0;
+    for (long long b = 0; b < B; ++b) acc += x[b * C + c];
+    out[c] = beta * out[c] + (float)acc;
+}
+
 __global__ void k_channel_sum(float* out, const float* x, long long B, long long C, long long S, float beta) {
     const long long c = blockIdx.x;
-    double acc = 0.0;
-    for (long long b = 0; b < B; ++b)
-        for (long long s = threadIdx.x; s < S; s += blockDim.x) acc += x[(b * C + c) * S + s];
+    const long long bd = blockDim.x;
+    double a[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) a[q] = 0.0;
+    for (long long b = 0; b < B; ++b) {
+        const float* row = x + (b * C + c) * S;
+        long long s = threadIdx.x;
+        for (; s + 7 * bd < S; s += 8 * bd) {
+#pragma unroll
+            for (int q = 0; q < 8; ++q) a[q] += row[s + q * bd];
+        }
+        for (; s < S; s += bd) a[0] += row[s];
+    }
+    const double acc = ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
     __shared__ double red[256];
     red[threadIdx.x] = acc;
     __syncthreads();
@@ -214,7 +236,12 @@ __global__ void k_rbig_fold(const float* drb, float* drr, float* dri, long long 
 // The mbarrier wait is bounded; on expiry the CTA sets *err and skips its
 // stores (the accumulator is freed either way).
 namespace tc {
-constexpr int TN = 256;      // columns of n per CTA (accumulator width)
+// columns of n per CTA (accumulator width); the TMEM it takes (TN columns
+// of 512) bounds the CTAs resident per SM
+#ifndef FNO_DENSE_TN
+#define FNO_DENSE_TN 128
+#endif
+constexpr int TN = FNO_DENSE_TN;
 constexpr int TM = 128;      // accumulator rows (M padded)
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }

@@ -112,6 +112,12 @@ def _grouped_instances():
         p["gamma"] = tuple(rng.uniform(0, 2, 2))
         if spin == 1:
             p["tau"] = (float(rng.uniform(200, 4000)), float(rng.uniform(-0.05, 0.05) * 2000), 0.0)
+            if not imag:
+                # real time at c0 ~ 4000 from this noisy start is unstable: the
+                # oracle amplifies a 1e-15 change of the start to 6e-7 in 12
+                # steps, so separately compiled kernels (FMA contraction) could
+                # not agree to rounding; a tenth of the coupling grows it to 5e-15
+                p["tau"] = (p["tau"][0] / 10, p["tau"][1] / 10, 0.0)
         p["alpha"] = (1.0, float(rng.uniform(1, 2)), 1.0)
         p["d"] = (25.6 / n[0], 25.6 / n[1])
         p["precision"] = prec

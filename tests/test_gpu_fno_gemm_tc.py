@@ -4,8 +4,8 @@ a PyTorch FP64 product of the same FP32 operands.  The cases follow the
 learned guess's spectral stages: a DFT matrix shared by every channel plane
 (the folded tall GEMM, and the transposed one when the shared matrix is the
 left operand), the per-mode channel mix with BF16 weights, the long-K weight
-gradient, column-major operands with M and N past one tile, and beta
-accumulation.  Bound: |C - C_ref| <= 1e-4 (|A| |B|) elementwise (the dropped
+gradient, column-major operands with M and N past one tile, beta
+accumulation, and ragged K and N ends of the float4 operand reads.  Bound: |C - C_ref| <= 1e-4 (|A| |B|) elementwise (the dropped
 lo*lo term and the tail roundings are about 2^-16 of each product)."""
 import ctypes
 
@@ -24,6 +24,8 @@ CASES = {
     "column-major-two-tiles": (1, 200, 300, 70, (0, 1, 200), (0, 300, 1), (0, 1, 200), 0, 1.0, 0.0),
     "interleaved-output": (16, 64, 64, 16, (64 * 16 * 2, 16, 1), (0, 64, 1), (64 * 64, 64, 1), 0, 1.0 / 4096, 1.0),
     "one-element": (1, 1, 1, 1, (0, 1, 1), (0, 1, 1), (0, 1, 1), 0, 2.0, 0.0),
+    "ragged-k-vectors": (3, 50, 20, 70, (50 * 72, 72, 1), (0, 20, 1), (50 * 20, 20, 1), 0, 1.0, 0.0),
+    "ragged-k-along-k": (2, 40, 36, 70, (40 * 72, 72, 1), (72 * 36, 1, 72), (40 * 36, 36, 1), 0, 1.0, 0.0),
 }
 
 
