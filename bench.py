@@ -286,12 +286,17 @@ def capture(args):
         for i, p in enumerate(insts):
             b[i].set_state(gaussian_nd(p))
             b[i].normt()
-        b.mode(grouped=True)
+        if args.batch_mode == "persistent":
+            b.mode(persistent=True)
+            b.variant(max(args.variant, 0))
+        else:
+            b.mode(grouped=True)
         b.config(32, 4)
         b.step(args.warmup + args.steps)
         obs = b.observables(with_conv=False)
         assert all(np.isfinite(o["en"]) for o in obs)
-        print(json.dumps({"capture": "sweep-grouped-32", "steps": args.warmup + args.steps}))
+        print(json.dumps({"capture": "sweep-%s-32" % ("persistent" if args.batch_mode == "persistent" else "grouped"),
+                          "steps": args.warmup + args.steps}))
         return
     w = WORKLOADS[args.workload]
     if w is D3:
@@ -692,9 +697,13 @@ def sweep(args):
     for i, p in enumerate(insts):
         b[i].set_state(gaussian_nd(p))
         b[i].normt()
-    tune = b.autotune(trial_steps=4, cache_path=os.path.join(out_dir(), "autotune_cache.txt"))
+    cache = os.path.join(out_dir(), "autotune_cache.txt")
+    tune = b.autotune(trial_steps=4, cache_path=cache)
+    tuned_mode = {0: "branches", 1: "grouped", 2: "persistent"}.get(int(open(cache).read().split()[-2]), "?")
     if args.batch_mode != "auto":
-        b.mode(grouped=args.batch_mode == "grouped")
+        b.mode(grouped=args.batch_mode == "grouped", persistent=args.batch_mode == "persistent")
+        if args.batch_mode == "persistent" and args.variant >= 0:
+            b.variant(args.variant)
         b.config(tune[0], tune[1])
     npts = sum(int(np.prod(p["n"])) for p in insts)
     b.step(max(args.warmup, 4))
@@ -711,7 +720,9 @@ def sweep(args):
            "dtype": "c128" if prec == "fp64" else "c64", "data": "synthetic (seeded parameter box, seed 4)",
            "config": {"workload": "sweep-512-ragged-q2d-spin1-imag", "instances": len(insts),
                       "sizes": sorted(set(p["n"][0] for p in insts)), "precision": prec,
-                      "autotuned": {"width": tune[0], "steps_per_graph": tune[1]}, "batch_mode": args.batch_mode,
+                      "autotuned": {"width": tune[0], "steps_per_graph": tune[1], "mode": tuned_mode,
+                                    "variant": b.variant(), "variant_shape": Batch.variant_shapes()[b.variant()]},
+                      "batch_mode": args.batch_mode,
                       "l2": "batch state larger than L2"},
            "roofline": {"bound": "hbm", "kernel": "whole batch step", "achieved": alg / (el / steps) / 1e9,
                         "peak": peak, "unit": "GB/s", "frac": alg / (el / steps) / 1e9 / peak,
@@ -796,8 +807,11 @@ def main():
     ap.add_argument("--grid", type=int, default=0, help="with --capture --workload 3d: points per axis (192)")
     ap.add_argument("--observables", action="store_true", help="with --capture: also run ENERGY/RAD (k_obs)")
     ap.add_argument("--fno3d", default=None, help="with --workload tts: saved 3D network parameters (.npz)")
-    ap.add_argument("--batch-mode", default="auto", choices=["auto", "grouped", "branches"],
-                    help="with --workload sweep: the autotuner's choice, or force grouped / per-instance branches")
+    ap.add_argument("--batch-mode", default="auto", choices=["auto", "grouped", "branches", "persistent"],
+                    help="with --workload sweep: the autotuner's choice, or force grouped / per-instance branches / "
+                         "one persistent launch")
+    ap.add_argument("--variant", type=int, default=-1,
+                    help="with --batch-mode persistent: the persistent kernel variant (default: the autotuner's)")
     ap.add_argument("--tts-max-steps", type=int, default=60000, help="with --workload tts: steps per FP64 stage")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

@@ -20,6 +20,7 @@ FGPE_E_CUDA = -2
 FGPE_E_STATE = -3
 FGPE_E_NONFINITE = -4
 FGPE_E_NEWTON = -5
+FGPE_E_TIMEOUT = -6
 
 FGPE_FP64 = 0
 FGPE_FP32 = 1
@@ -27,6 +28,7 @@ FGPE_STEP_DEFAULT = 0
 FGPE_STEP_NO_SNAPSHOT = 1
 FGPE_BATCH_BRANCHES = 0
 FGPE_BATCH_GROUPED = 1
+FGPE_BATCH_PERSISTENT = 2
 
 OPS = {"FFT": 1, "KE": 2, "SOC": 3, "BFT": 4, "SE": 5, "SP": 6}
 
@@ -41,7 +43,8 @@ EXPORTS = (
     "fgpe_batch_last_error", "fgpe_batch_config", "fgpe_batch_step", "fgpe_batch_observables",
     "fgpe_batch_autotune", "fgpe_batch_tuning", "fgpe_set_kernels", "fgpe_normc_noalloc",
     "fgpe_checkpoint_save", "fgpe_checkpoint_load", "fgpe_batch_step_timed", "fgpe_norms_sink",
-    "fgpe_fp64_fma_rate", "fgpe_batch_mode",
+    "fgpe_fp64_fma_rate", "fgpe_batch_mode", "fgpe_batch_variant", "fgpe_batch_variant_shape",
+    "fgpe_batch_variants", "fgpe_batch_wait_bound",
 )
 
 
@@ -115,6 +118,10 @@ def load():
         "fgpe_checkpoint_load": ([vp, ctypes.c_char_p, ctypes.POINTER(ctypes.c_longlong), dp], ip),
         "fgpe_fp64_fma_rate": ([ip, dp], ip),
         "fgpe_batch_mode": ([vp, ip], ip),
+        "fgpe_batch_variant": ([vp, ip, ctypes.POINTER(ip)], ip),
+        "fgpe_batch_variant_shape": ([ip, ctypes.POINTER(ip)], ip),
+        "fgpe_batch_variants": ([], ip),
+        "fgpe_batch_wait_bound": ([vp, ctypes.c_double, ip], ip),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

@@ -54,12 +54,44 @@ class Batch:
     def config(self, width=0, steps_per_graph=0):
         check_batch(self._L.fgpe_batch_config(self._b, int(width), int(steps_per_graph)), self._b)
 
-    def mode(self, grouped):
+    def mode(self, grouped=False, persistent=False):
         """grouped=True: instances sharing a q2D grid shape advance together,
-        one column-pass and one row-pass launch per step per group
-        (fgpe_batch_mode); False: one graph branch per instance."""
-        m = _abi.FGPE_BATCH_GROUPED if grouped else _abi.FGPE_BATCH_BRANCHES
+        one column-pass and one row-pass launch per step per group;
+        persistent=True: every q2D instance of a size-specialised grid (one
+        spin and precision) advances by one persistent kernel launch per
+        graph of steps; neither: one graph branch per instance
+        (fgpe_batch_mode)."""
+        if persistent:
+            m = _abi.FGPE_BATCH_PERSISTENT
+        else:
+            m = _abi.FGPE_BATCH_GROUPED if grouped else _abi.FGPE_BATCH_BRANCHES
         check_batch(self._L.fgpe_batch_mode(self._b, m), self._b)
+
+    def variant(self, v=-1):
+        """Select the persistent kernel variant v (v < 0: keep it); returns
+        the current one (fgpe_batch_variant)."""
+        cur = ctypes.c_int()
+        check_batch(self._L.fgpe_batch_variant(self._b, int(v), ctypes.byref(cur)), self._b)
+        return cur.value
+
+    @staticmethod
+    def variant_shapes():
+        """Shapes of the persistent kernel variants: dicts of threads per
+        block, values per row tile, bytes of x per column tile row and the
+        radix plan of the y lines (fgpe_batch_variant_shape)."""
+        L = _abi.load()
+        out = []
+        for v in range(L.fgpe_batch_variants()):
+            sh = (ctypes.c_int * 4)()
+            check_batch(L.fgpe_batch_variant_shape(v, sh))
+            out.append(dict(threads=sh[0], row_values=sh[1], col_bytes=sh[2], y_plan=sh[3]))
+        return out
+
+    def wait_bound(self, wait_ms, stall_instance=-1):
+        """Bound on one device-side wait of the persistent kernel, in ms;
+        stall_instance >= 0 makes that instance's first wait run out (a test
+        of the error path: the next step raises FgpeError FGPE_E_TIMEOUT)."""
+        check_batch(self._L.fgpe_batch_wait_bound(self._b, float(wait_ms), int(stall_instance)), self._b)
 
     def tuning(self):
         w, k = ctypes.c_int(), ctypes.c_int()

@@ -11,7 +11,8 @@ def build(verbose=False):
     # use the toolchain on PATH (nvcc drives the host compiler itself)
     env.pop("CC", None)
     env.pop("CXX", None)
-    cmd = ["make", "-C", os.path.join(HERE, "csrc")]
+    # the translation units compile in parallel (the largest takes minutes)
+    cmd = ["make", "-j", str(max(2, min(8, os.cpu_count() or 2))), "-C", os.path.join(HERE, "csrc")]
     if not verbose:
         cmd.insert(1, "-s")
     subprocess.run(cmd, check=True, env=env)

@@ -21,6 +21,7 @@
 #include "fgpe_kernels.cuh"
 #include "fgpe_fast.cuh"
 #include "fgpe_group.cuh"
+#include "fgpe_persist.h"
 #include "fno_kernels.cuh"
 #include "fno_gemm_tc.cuh"
 #include "../../include/fno.h"
@@ -1402,11 +1403,35 @@ struct BatchGroup {
     int row_tiles = 0, chunk = 0, col_tiles = 0, row_grid = 0, col_grid = 0;
 };
 
+// Persistent mode: the instances of one spin and precision that the
+// persistent kernel covers (fgpe_persist.cuh), advanced by one launch per
+// captured graph.
+struct PersistSet {
+    int ms = 0, fp32 = 0;
+    std::vector<int> members;
+    PInst* d_inst = nullptr;         // per-instance table (device)
+    PInst* h_inst = nullptr;         // pinned staging of the table
+    unsigned* d_items = nullptr;     // one step's items: column tiles, then row chunks
+    int ncol = 0, nrow = 0;
+    double* part = nullptr;          // NORMC chunk partials
+    std::vector<size_t> part_off;    // per member, in doubles
+    unsigned* sync = nullptr;        // 3 counters per member, then PCTL_LEN control words
+    int* ymaps = nullptr;            // y position maps of the variant's plan
+    std::vector<std::pair<int, size_t>> ymap_off;   // (ny, offset)
+    std::vector<int> col_tiles, row_tiles, chunk;
+    size_t smem = 0;
+    int grid = 0;
+};
+
 struct fgpe_batch_s {
     std::vector<fgpe_t*> inst;
     int mode = FGPE_BATCH_BRANCHES;
     std::vector<BatchGroup> groups;         // grouped mode: instances sharing launches
-    std::vector<int> loose;                 // grouped mode: instances on their own branches
+    std::vector<PersistSet> psets;          // persistent mode: one kernel per set
+    int pvariant = 0;                       // persistent mode: kernel variant (kPersistShapes)
+    double wait_ms = 2000.0;                // persistent mode: bound on one device-side wait
+    int stall = -1;                         // persistent mode, tests: instance whose first wait cannot end
+    std::vector<int> loose;                 // grouped/persistent mode: instances on their own branches
     cudaStream_t origin = nullptr;
     std::vector<cudaStream_t> lanes;
     std::vector<cudaEvent_t> ev;            // fork/join events, one per lane + 1
@@ -1678,6 +1703,245 @@ int capture_grouped(fgpe_batch_t* b, int nsteps) {
     return FGPE_OK;
 }
 
+// ------------------------------------------------------- persistent mode
+void free_psets(fgpe_batch_t* b) {
+    for (PersistSet& p : b->psets) {
+        if (p.d_inst) cudaFree(p.d_inst);
+        if (p.h_inst) cudaFreeHost(p.h_inst);
+        if (p.d_items) cudaFree(p.d_items);
+        if (p.part) cudaFree(p.part);
+        if (p.sync) cudaFree(p.sync);
+        if (p.ymaps) cudaFree(p.ymaps);
+    }
+    b->psets.clear();
+    b->loose.clear();
+}
+
+template <typename T, int MS> int pset_prepare(PersistSet& p, int variant, int nmask) {
+    const PersistShape& sh = kPersistShapes[variant];
+    p.smem = persist_smem<T, MS>(sh.rn, sh.txb, nmask);
+    int bps = 0;
+    cudaError_t e = persist_prepare<T, MS>(variant, p.smem, &bps);
+    if (e != cudaSuccess) return FGPE_E_CUDA;
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    p.grid = bps * sms;
+    return p.grid > 0 ? FGPE_OK : FGPE_E_ARG;
+}
+
+// Sort the instances into persistent sets (q2D, size-specialised kernels on
+// both axes; one set per spin and precision) and instances that keep their
+// own graph branches; build each set's item list, y maps and counters.
+int build_psets(fgpe_batch_t* b) {
+    free_groups(b);
+    free_psets(b);
+    const PersistShape& sh = kPersistShapes[b->pvariant];
+    const int fast_ns[5] = {128, 192, 256, 384, 512};
+    for (int i = 0; i < (int)b->inst.size(); ++i) {
+        fgpe_t* h = b->inst[i];
+        const bool ok = h->p.dim == 2 && h->fast_row && h->fast_col[1] && fast_size(h->p.nx) && fast_size(h->p.ny);
+        if (!ok) { b->loose.push_back(i); continue; }
+        PersistSet* p = nullptr;
+        for (PersistSet& q : b->psets)
+            if (q.ms == h->ms && q.fp32 == h->fp32) p = &q;
+        if (!p) {
+            b->psets.emplace_back();
+            p = &b->psets.back();
+            p->ms = h->ms; p->fp32 = h->fp32;
+        }
+        p->members.push_back(i);
+    }
+    for (PersistSet& p : b->psets) {
+        const int n = (int)p.members.size();
+        if (n > 65535) { free_psets(b); return bfail(b, FGPE_E_ARG, "persistent batch: more than 65535 instances in one set"); }
+        const int cs = p.fp32 ? 8 : 16;
+        const int tx = sh.txb / cs;
+        int nmask = 0;
+        std::vector<unsigned> col_items, row_items;
+        size_t nparts = 0;
+        for (int k = 0; k < n; ++k) {
+            const fgpe_t* h = b->inst[p.members[k]];
+            const int r = prow_r(sh.rn, h->p.nx);
+            if (tx < 1 || h->p.nx % tx || h->p.ny % r) {
+                free_psets(b);
+                return bfail(b, FGPE_E_ARG, "persistent batch: grid not divisible by the variant's tiles");
+            }
+            for (int z = 0; z < 5; ++z) if (h->p.nx == fast_ns[z] || h->p.ny == fast_ns[z]) nmask |= 1 << z;
+            const int ct = h->p.nx / tx, rt = h->p.ny / r;
+            int ch = 1;
+            for (int d = 1; d <= 4; ++d) if (rt % d == 0) ch = d;
+            p.col_tiles.push_back(ct);
+            p.row_tiles.push_back(rt);
+            p.chunk.push_back(ch);
+            for (int t = 0; t < ct; ++t) col_items.push_back(((unsigned)k << 16) | (unsigned)t);
+            for (int c = 0; c < rt / ch; ++c) row_items.push_back(((unsigned)k << 16) | (unsigned)c);
+            p.part_off.push_back(nparts);
+            nparts += (size_t)(rt / ch) * p.ms;
+            bool have = false;
+            for (auto& yo : p.ymap_off) have = have || yo.first == h->p.ny;
+            if (!have) p.ymap_off.push_back({h->p.ny, 0});
+        }
+        p.ncol = (int)col_items.size();
+        p.nrow = (int)row_items.size();
+        std::vector<unsigned> items(col_items);
+        items.insert(items.end(), row_items.begin(), row_items.end());
+        // y maps of the variant's radix plan (the x layout stays the handle's)
+        std::vector<int> ym;
+        for (auto& yo : p.ymap_off) {
+            const CPlan cp = cplan(yo.first, sh.pv);
+            FftPlan pl;
+            pl.n = yo.first; pl.nf = cp.nf;
+            for (int f = 0; f < cp.nf; ++f) pl.r[f] = cp.r[f];
+            yo.second = ym.size();
+            std::vector<int> f = position_map(pl);
+            ym.insert(ym.end(), f.begin(), f.end());
+        }
+        int r = p.fp32 ? (p.ms == 3 ? pset_prepare<float, 3>(p, b->pvariant, nmask) : pset_prepare<float, 5>(p, b->pvariant, nmask))
+                       : (p.ms == 3 ? pset_prepare<double, 3>(p, b->pvariant, nmask) : pset_prepare<double, 5>(p, b->pvariant, nmask));
+        if (r) { free_psets(b); return bfail(b, r, "persistent batch: the kernel variant does not fit the device"); }
+        BCK(cudaMalloc(&p.d_inst, n * sizeof(PInst)));
+        BCK(cudaMallocHost(&p.h_inst, n * sizeof(PInst)));
+        BCK(cudaMalloc(&p.d_items, items.size() * sizeof(unsigned)));
+        BCK(cudaMemcpy(p.d_items, items.data(), items.size() * sizeof(unsigned), cudaMemcpyHostToDevice));
+        BCK(cudaMalloc(&p.part, nparts * sizeof(double)));
+        BCK(cudaMalloc(&p.sync, (3 * (size_t)n + PCTL_LEN) * sizeof(unsigned)));
+        BCK(cudaMemset(p.sync, 0, (3 * (size_t)n + PCTL_LEN) * sizeof(unsigned)));
+        BCK(cudaMalloc(&p.ymaps, ym.size() * sizeof(int)));
+        BCK(cudaMemcpy(p.ymaps, ym.data(), ym.size() * sizeof(int), cudaMemcpyHostToDevice));
+    }
+    return FGPE_OK;
+}
+
+// Instance tables from the handles' current buffers and constants, copied
+// ahead of the graph launch on the batch's launch stream.
+int refresh_pinst(fgpe_batch_t* b) {
+    for (PersistSet& p : b->psets) {
+        for (size_t k = 0; k < p.members.size(); ++k) {
+            fgpe_t* h = b->inst[p.members[k]];
+            PInst& q = p.h_inst[k];
+            q.d.c = h->sc;
+            q.d.S = h->S; q.d.psi = h->psi; q.d.prev = h->prev;
+            q.d.info = h->info; q.d.info_prev = h->info_prev;
+            q.d.part = p.part + p.part_off[k];
+            q.d.counter = nullptr;
+            q.fy = nullptr;
+            for (auto& yo : p.ymap_off) if (yo.first == h->p.ny) q.fy = p.ymaps + yo.second;
+            q.col_tiles = p.col_tiles[k];
+            q.row_tiles = p.row_tiles[k];
+            q.chunk = p.chunk[k];
+        }
+        BCK(cudaMemcpyAsync(p.d_inst, p.h_inst, p.members.size() * sizeof(PInst), cudaMemcpyHostToDevice, b->origin));
+    }
+    return FGPE_OK;
+}
+
+// Persistent mode capture: per set, the counters cleared and one kernel
+// launch for all nsteps; the remaining instances as their own branches.
+int capture_persistent(fgpe_batch_t* b, int nsteps) {
+    drop_graph(b);
+    int r = build_psets(b);
+    if (r) return r;
+    for (fgpe_t* h : b->inst) {
+        if (!h->has_state) return bfail(b, FGPE_E_STATE, "batch instance without a state");
+        if (h->p.dim >= 2 && !h->S_valid) {
+            DISPATCH(h, launch_row, h, ROW_FWD, nullptr);
+            BCK(cudaGetLastError());
+            h->S_valid = true;
+        }
+        BCK(cudaStreamSynchronize(h->st));
+    }
+    const int nbr = (int)b->psets.size() + (int)b->loose.size();
+    r = set_width(b, std::max(b->width, std::min(nbr, 64)));
+    if (r) return r;
+    r = refresh_pinst(b);
+    if (r) return r;
+    BCK(cudaStreamSynchronize(b->origin));
+    cudaGraph_t gr;
+    BCK(cudaStreamBeginCapture(b->origin, cudaStreamCaptureModeThreadLocal));
+    BCK(cudaEventRecord(b->ev[0], b->origin));
+    for (int l = 0; l < b->width; ++l) BCK(cudaStreamWaitEvent(b->lanes[l], b->ev[0], 0));
+    int lane = 0;
+    cudaError_t le = cudaSuccess;
+    for (const PersistSet& p : b->psets) {
+        cudaStream_t st = b->lanes[lane++ % b->width];
+        const int n = (int)p.members.size();
+        if (le == cudaSuccess) le = cudaMemsetAsync(p.sync, 0, (3 * (size_t)n + PCTL_LEN) * sizeof(unsigned), st);
+        PersistArgs a;
+        a.inst = p.d_inst;
+        a.items = p.d_items;
+        a.ncol = p.ncol;
+        a.nrow = p.nrow;
+        a.nsteps = nsteps;
+        a.sync = p.sync;
+        a.ctl = p.sync + 3 * (size_t)n;
+        a.wait_ns = (long long)(b->wait_ms * 1e6);
+        a.ninst = n;
+        a.stall = -1;
+        for (int k = 0; k < n; ++k) if (p.members[k] == b->stall) a.stall = k;
+        if (le == cudaSuccess)
+            le = p.fp32 ? (p.ms == 3 ? persist_launch<float, 3>(b->pvariant, a, p.grid, p.smem, st)
+                                     : persist_launch<float, 5>(b->pvariant, a, p.grid, p.smem, st))
+                        : (p.ms == 3 ? persist_launch<double, 3>(b->pvariant, a, p.grid, p.smem, st)
+                                     : persist_launch<double, 5>(b->pvariant, a, p.grid, p.smem, st));
+        for (int i : p.members) {
+            fgpe_t* h = b->inst[i];
+            h->S_valid = true; h->psi_valid = true; h->prev_valid = true; h->norms_valid = true;
+        }
+    }
+    for (int i : b->loose) {
+        fgpe_t* h = b->inst[i];
+        cudaStream_t keep = h->st;
+        const bool prof = h->prof;
+        h->st = b->lanes[lane++ % b->width];
+        h->prof = false;
+        const int rc = fgpe_step_ex(h, nsteps, FGPE_STEP_DEFAULT);
+        h->st = keep;
+        h->prof = prof;
+        if (rc) { cudaGraph_t junk; cudaStreamEndCapture(b->origin, &junk); if (junk) cudaGraphDestroy(junk); return rc; }
+    }
+    for (int l = 0; l < b->width; ++l) {
+        BCK(cudaEventRecord(b->ev[1 + l], b->lanes[l]));
+        BCK(cudaStreamWaitEvent(b->origin, b->ev[1 + l], 0));
+    }
+    cudaGraph_t junk = nullptr;
+    if (le != cudaSuccess) {
+        cudaStreamEndCapture(b->origin, &junk);
+        if (junk) cudaGraphDestroy(junk);
+        return bfail(b, FGPE_E_CUDA, std::string("persistent batch launch: ") + cudaGetErrorString(le));
+    }
+    BCK(cudaStreamEndCapture(b->origin, &gr));
+    cudaError_t e = cudaGraphInstantiate(&b->exec, gr, 0);
+    cudaGraphDestroy(gr);
+    BCK(e);
+    BCK(cudaGetLastError());
+    b->exec_steps = nsteps;
+    return FGPE_OK;
+}
+
+// After a synchronised persistent launch: a device-side wait that ran out
+// leaves its code in the set's control words.
+int check_psets(fgpe_batch_t* b) {
+    for (const PersistSet& p : b->psets) {
+        unsigned ctl[PCTL_LEN];
+        BCK(cudaMemcpy(ctl, p.sync + 3 * p.members.size(), sizeof(ctl), cudaMemcpyDeviceToHost));
+        if (ctl[PCTL_ERR] == PERR_NONE) continue;
+        const unsigned per = (unsigned)(p.ncol + p.nrow);
+        const unsigned r = per ? ctl[PCTL_WHERE] % per : 0;
+        unsigned e = 0;
+        BCK(cudaMemcpy(&e, p.d_items + r, sizeof(e), cudaMemcpyDeviceToHost));
+        const int k = (int)(e >> 16);
+        const int inst = k < (int)p.members.size() ? p.members[k] : -1;
+        b->exec_steps = 0;   // the states are not those of whole steps: capture afresh
+        drop_graph(b);
+        return bfail(b, FGPE_E_TIMEOUT,
+                     std::string("persistent batch: a device-side wait ran out (") +
+                         (ctl[PCTL_ERR] == PERR_WAIT_COL ? "column tile" : "row chunk") + " of instance " +
+                         std::to_string(inst) + ", step " + std::to_string(ctl[PCTL_STEP]) + " of the launch)");
+    }
+    return FGPE_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1705,6 +1969,7 @@ int fgpe_batch_destroy(fgpe_batch_t* b) {
     if (b->origin) cudaStreamSynchronize(b->origin);
     drop_graph(b);
     free_groups(b);
+    free_psets(b);
     for (cudaStream_t s : b->lanes) cudaStreamDestroy(s);
     for (cudaEvent_t e : b->ev) cudaEventDestroy(e);
     if (b->origin) cudaStreamDestroy(b->origin);
@@ -1753,15 +2018,25 @@ int fgpe_batch_step(fgpe_batch_t* b, int nsteps) {
             continue;
         }
         if (!b->exec || b->exec_steps != k) {
-            int r = b->mode == FGPE_BATCH_GROUPED ? capture_grouped(b, k) : capture(b, k);
+            int r = b->mode == FGPE_BATCH_GROUPED      ? capture_grouped(b, k)
+                    : b->mode == FGPE_BATCH_PERSISTENT ? capture_persistent(b, k)
+                                                       : capture(b, k);
             if (r) return r;
         } else if (b->mode == FGPE_BATCH_GROUPED) {
             int r = refresh_descs(b);
+            if (r) return r;
+        } else if (b->mode == FGPE_BATCH_PERSISTENT) {
+            int r = refresh_pinst(b);
             if (r) return r;
         }
         BCK(cudaGraphLaunch(b->exec, b->origin));
         for (fgpe_t* h : b->inst) h->launches += step_launches(h, k);
         left -= k;
+        if (b->mode == FGPE_BATCH_PERSISTENT) {
+            BCK(cudaStreamSynchronize(b->origin));
+            int r = check_psets(b);
+            if (r) return r;
+        }
     }
     BCK(cudaStreamSynchronize(b->origin));
     return FGPE_OK;
@@ -1784,8 +2059,12 @@ int fgpe_batch_step_timed(fgpe_batch_t* b, int nsteps, double* device_ms) {
     while (err == cudaSuccess && rc == FGPE_OK && left > 0) {
         int k = std::min(left, b->ksteps);
         if (k == 1) k = 2;   // cannot happen: remainder 1 rejected above
-        if (!b->exec || b->exec_steps != k) rc = b->mode == FGPE_BATCH_GROUPED ? capture_grouped(b, k) : capture(b, k);
+        if (!b->exec || b->exec_steps != k)
+            rc = b->mode == FGPE_BATCH_GROUPED      ? capture_grouped(b, k)
+                 : b->mode == FGPE_BATCH_PERSISTENT ? capture_persistent(b, k)
+                                                    : capture(b, k);
         else if (b->mode == FGPE_BATCH_GROUPED) rc = refresh_descs(b);
+        else if (b->mode == FGPE_BATCH_PERSISTENT) rc = refresh_pinst(b);
         if (rc) break;
         err = cudaGraphLaunch(b->exec, b->origin);
         for (fgpe_t* h : b->inst) h->launches += step_launches(h, k);
@@ -1799,6 +2078,10 @@ int fgpe_batch_step_timed(fgpe_batch_t* b, int nsteps, double* device_ms) {
     cudaEventDestroy(e1);
     if (rc) return rc;
     BCK(err);
+    if (b->mode == FGPE_BATCH_PERSISTENT) {
+        rc = check_psets(b);
+        if (rc) return rc;
+    }
     *device_ms = ms;
     return FGPE_OK;
 }
@@ -1854,17 +2137,19 @@ int fgpe_batch_autotune(fgpe_batch_t* b, int trial_steps, const char* cache_path
             while (fgets(line, sizeof line, f)) {
                 std::string l(line);
                 if (l.compare(0, sig.size() + 1, sig + " ") != 0) continue;
-                int w = 0, k = 0, md = FGPE_BATCH_BRANCHES;
+                int w = 0, k = 0, md = FGPE_BATCH_BRANCHES, pv = 0;
                 double tms = 0;
                 char fam[4096] = {0};
-                const int got = sscanf(l.c_str() + sig.size() + 1, "%d %d %4095s %lf %d", &w, &k, fam, &tms, &md);
+                const int got = sscanf(l.c_str() + sig.size() + 1, "%d %d %4095s %lf %d %d", &w, &k, fam, &tms, &md, &pv);
                 if (got >= 3) {
                     fclose(f);
                     std::string fs(fam);
                     for (size_t ci = 0; ci < classes.size() && ci < fs.size(); ++ci)
                         for (int i = 0; i < n; ++i)
                             if (sizes[i] == classes[ci]) fgpe_set_kernels(b->inst[i], fs[ci] == 'g' ? FGPE_KERNELS_GENERIC : FGPE_KERNELS_AUTO);
-                    const int rm = fgpe_batch_mode(b, got >= 5 ? md : FGPE_BATCH_BRANCHES);
+                    int rm = fgpe_batch_variant(b, got >= 6 ? pv : 0, nullptr);
+                    if (rm) return rm;
+                    rm = fgpe_batch_mode(b, got >= 5 ? md : FGPE_BATCH_BRANCHES);
                     if (rm) return rm;
                     return fgpe_batch_config(b, w, k);
                 }
@@ -1975,6 +2260,27 @@ int fgpe_batch_autotune(fgpe_batch_t* b, int trial_steps, const char* cache_path
             if (r) return finish(r);
             if (ms < best_ms) { best_ms = ms; bw = std::min(n, 64); bk = k; bmode = FGPE_BATCH_GROUPED; }
         }
+    }
+    // 4) one persistent launch per graph for all covered instances, for every
+    //    kernel variant (threads per block, rows per row tile, bytes per
+    //    column tile row, radix plan of the y lines)
+    int bvar = b->pvariant;
+    {
+        int r = fgpe_batch_mode(b, FGPE_BATCH_PERSISTENT);
+        if (r) return finish(r);
+        for (int v = 0; v < kPersistVariants; ++v) {
+            r = fgpe_batch_variant(b, v, nullptr);
+            if (r) return finish(r);
+            for (int k : ks) {
+                double ms = 0;
+                r = timed(std::min(n, 64), k, &ms);
+                if (r == FGPE_E_ARG) break;   // this variant's tiles do not fit the batch
+                if (r) return finish(r);
+                if (ms < best_ms) { best_ms = ms; bw = std::min(n, 64); bk = k; bmode = FGPE_BATCH_PERSISTENT; bvar = v; }
+            }
+        }
+        r = fgpe_batch_variant(b, bvar, nullptr);
+        if (r) return finish(r);
         r = fgpe_batch_mode(b, bmode);
         if (r) return finish(r);
     }
@@ -1985,19 +2291,58 @@ int fgpe_batch_autotune(fgpe_batch_t* b, int trial_steps, const char* cache_path
     if (r) return r;
     if (cache_path) {
         FILE* f = fopen(cache_path, "a");
-        if (f) { fprintf(f, "%s %d %d %s %.6f %d\n", sig.c_str(), bw, bk, fam.c_str(), best_ms, bmode); fclose(f); }
+        if (f) {
+            fprintf(f, "%s %d %d %s %.6f %d %d\n", sig.c_str(), bw, bk, fam.c_str(), best_ms, bmode, bvar);
+            fclose(f);
+        }
     }
     return FGPE_OK;
 }
 
 int fgpe_batch_mode(fgpe_batch_t* b, int mode) {
     if (!b) return bfail(b, FGPE_E_ARG, "null batch");
-    if (mode != FGPE_BATCH_BRANCHES && mode != FGPE_BATCH_GROUPED) return bfail(b, FGPE_E_ARG, "unknown batch mode");
+    if (mode != FGPE_BATCH_BRANCHES && mode != FGPE_BATCH_GROUPED && mode != FGPE_BATCH_PERSISTENT)
+        return bfail(b, FGPE_E_ARG, "unknown batch mode");
     if (mode != b->mode) {
         drop_graph(b);
         free_groups(b);
+        free_psets(b);
         b->mode = mode;
     }
+    return FGPE_OK;
+}
+
+int fgpe_batch_variant(fgpe_batch_t* b, int variant, int* current) {
+    if (!b) return bfail(b, FGPE_E_ARG, "null batch");
+    if (variant >= kPersistVariants) return bfail(b, FGPE_E_ARG, "unknown persistent kernel variant");
+    if (variant >= 0 && variant != b->pvariant) {
+        drop_graph(b);
+        free_psets(b);
+        b->pvariant = variant;
+    }
+    if (current) *current = b->pvariant;
+    return FGPE_OK;
+}
+
+int fgpe_batch_variants(void) { return kPersistVariants; }
+
+int fgpe_batch_variant_shape(int variant, int* shape) {
+    if (variant < 0 || variant >= kPersistVariants || !shape) return FGPE_E_ARG;
+    const PersistShape& s = kPersistShapes[variant];
+    shape[0] = s.th;
+    shape[1] = s.rn;
+    shape[2] = s.txb;
+    shape[3] = s.pv;
+    return FGPE_OK;
+}
+
+int fgpe_batch_wait_bound(fgpe_batch_t* b, double wait_ms, int stall_instance) {
+    if (!b) return bfail(b, FGPE_E_ARG, "null batch");
+    if (!(wait_ms > 0.0) || wait_ms > 600000.0) return bfail(b, FGPE_E_ARG, "wait bound must be in (0, 600000] ms");
+    if (stall_instance < -1 || stall_instance >= (int)b->inst.size()) return bfail(b, FGPE_E_ARG, "bad instance index");
+    b->wait_ms = wait_ms;
+    b->stall = stall_instance;
+    drop_graph(b);
     return FGPE_OK;
 }
 

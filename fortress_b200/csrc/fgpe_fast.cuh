@@ -18,17 +18,29 @@ struct CPlan {
     int nf;
     int r[12];
 };
-constexpr CPlan cplan(int n) {
+// Radix plans.  pv = 0: radix 8 while it divides, then one 4 or 2, then
+// 3s and 5s (the plan of every kernel and of the handle's spectral layout).
+// pv = 1: as 0, but a trailing 8*2 pair becomes 4*4 (no radix-2 pass).
+// pv = 2: the radices of plan 0 in reverse order (small radices on the
+// longest stride).  Only transforms whose spectra stay inside one kernel
+// (the y lines of the persistent batch kernel) use pv != 0.
+constexpr CPlan cplan(int n, int pv = 0) {
     CPlan p{0, {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0}};
     while (n % 8 == 0) { p.r[p.nf++] = 8; n /= 8; }
     if (n % 4 == 0) { p.r[p.nf++] = 4; n /= 4; }
-    if (n % 2 == 0) { p.r[p.nf++] = 2; n /= 2; }
+    if (n % 2 == 0) {
+        if (pv == 1 && p.nf > 0 && p.r[p.nf - 1] == 8) { p.r[p.nf - 1] = 4; p.r[p.nf++] = 4; }
+        else p.r[p.nf++] = 2;
+        n /= 2;
+    }
     while (n % 3 == 0) { p.r[p.nf++] = 3; n /= 3; }
     while (n % 5 == 0) { p.r[p.nf++] = 5; n /= 5; }
+    if (pv == 2)
+        for (int i = 0, j = p.nf - 1; i < j; ++i, --j) { const int t = p.r[i]; p.r[i] = p.r[j]; p.r[j] = t; }
     return p;
 }
-constexpr int cplan_block(int n, int pass) {
-    CPlan pl = cplan(n);
+constexpr int cplan_block(int n, int pass, int pv = 0) {
+    CPlan pl = cplan(n, pv);
     int b = n;
     for (int i = 0; i < pass; ++i) b /= pl.r[i];
     return b;
@@ -63,17 +75,21 @@ template <int N, int TX> struct ColTile {
 // the radix of the next pass of the same transform, 0 after the last.
 // WARP = 1: the lines belong to one warp (TH = 32, tasks by lane) and every
 // pass ends on __syncwarp.
-template <typename T, bool INV, int N, int NL, int TH, int P, class Map, int NEXT_R = 0, int WARP = 0>
+template <typename T, bool INV, int N, int NL, int TH, int P, class Map, int NEXT_R = 0, int WARP = 0, int PV = 0,
+          int UMAX = 0>
 __device__ __forceinline__ void ct_pass(cx<T>* s, const cx<T>* __restrict__ tw) {
-    constexpr CPlan pl = cplan(N);
+    constexpr CPlan pl = cplan(N, PV);
     constexpr int R = pl.r[P];
-    constexpr int BP = cplan_block(N, P);
+    constexpr int BP = cplan_block(N, P, PV);
     constexpr int SI = BP / R, NB = N / R, TOT = NL * NB, ITER = (TOT + TH - 1) / TH, TSTEP = N / BP;
     constexpr int GT = Map::GROUP(NB);
     constexpr bool GROUPED = NEXT_R == R && TOT == TH && GT % 32 == 0 && TOT % GT == 0 && TOT / GT <= 15;
     static_assert(!WARP || TH == 32, "warp-scope passes run on 32 lanes");
     const int tid = WARP ? (int)(threadIdx.x & 31) : (int)threadIdx.x;
-#pragma unroll
+    // UMAX > 0: passes of more than UMAX tasks per thread stay rolled (the
+    // register budget of kernels that hold several line lengths)
+    constexpr int UNR = (UMAX == 0 || ITER <= UMAX) ? ITER : 1;
+#pragma unroll UNR
     for (int it = 0; it < ITER; ++it) {
         const int b = tid + it * TH;
         if ((TOT % TH) == 0 || b < TOT) {
@@ -114,21 +130,21 @@ __device__ __forceinline__ void ct_pass(cx<T>* s, const cx<T>* __restrict__ tw) 
     }
 }
 
-template <typename T, bool INV, int N, int NL, int TH, class Map, int WARP = 0, int P = 0>
+template <typename T, bool INV, int N, int NL, int TH, class Map, int WARP = 0, int P = 0, int PV = 0, int UMAX = 0>
 __device__ __forceinline__ void ct_fft(cx<T>* s, const cx<T>* __restrict__ tw) {
-    constexpr CPlan pl = cplan(N);
+    constexpr CPlan pl = cplan(N, PV);
     if constexpr (P < pl.nf) {
         constexpr int PP = INV ? pl.nf - 1 - P : P;
         constexpr int NEXT_R = P + 1 < pl.nf ? pl.r[INV ? PP - 1 : PP + 1] : 0;
-        ct_pass<T, INV, N, NL, TH, PP, Map, NEXT_R, WARP>(s, tw);
-        ct_fft<T, INV, N, NL, TH, Map, WARP, P + 1>(s, tw);
+        ct_pass<T, INV, N, NL, TH, PP, Map, NEXT_R, WARP, PV, UMAX>(s, tw);
+        ct_fft<T, INV, N, NL, TH, Map, WARP, P + 1, PV, UMAX>(s, tw);
     }
 }
 
 // ------------------------------------------------------------- cp.async
 #ifdef FGPE_CHECK_ALIGN
 // Diagnostic build only: record the first misaligned copy and skip it.
-__device__ unsigned long long g_align_fault[4];
+static __device__ unsigned long long g_align_fault[4];
 __device__ __forceinline__ bool align_bad(const void* s, const void* g, unsigned bytes, int site) {
     const unsigned d = (unsigned)__cvta_generic_to_shared(s);
     if ((d % bytes) == 0 && ((unsigned long long)g % bytes) == 0) return false;

@@ -857,7 +857,7 @@ __global__ void k_apply_scale(T* psi, long long n2, long long per2, double* info
 // device memory or pinned host memory that the device addresses directly.  As
 // a programmatic dependent launch it waits for the step's last pass and keeps
 // the step chain on the SMs instead of a copy-engine transfer between steps.
-__global__ void k_norms_out(const double* __restrict__ info, double* __restrict__ dst, int ms) {
+static __global__ void k_norms_out(const double* __restrict__ info, double* __restrict__ dst, int ms) {
     asm volatile("griddepcontrol.wait;\n" ::: "memory");
     if ((int)threadIdx.x < ms) dst[threadIdx.x] = info[INFO_NORM + threadIdx.x];
 }

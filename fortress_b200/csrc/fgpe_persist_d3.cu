@@ -1,0 +1,6 @@
+// Persistent batch kernel, double complex, spin 1 (fgpe_persist.cuh).
+#include "fgpe_persist_impl.cuh"
+
+namespace fgpe {
+FGPE_PERSIST_INSTANTIATE(double, 3)
+}  // namespace fgpe

@@ -36,8 +36,11 @@ enum {
     FGPE_E_CUDA = -2,       /* CUDA runtime error (message in fgpe_last_error) */
     FGPE_E_STATE = -3,      /* call out of order (e.g. no state set) */
     FGPE_E_NONFINITE = -4,  /* a reduction produced NaN/Inf */
-    FGPE_E_NEWTON = -5      /* spin-2 magnetisation projection: Newton-Raphson
+    FGPE_E_NEWTON = -5,     /* spin-2 magnetisation projection: Newton-Raphson
                                did not converge (cgpe1d.f90:1287-1290) */
+    FGPE_E_TIMEOUT = -6     /* a bounded device-side wait of the persistent
+                               batch kernel ran out; the batch's states are
+                               not those of whole steps */
 };
 
 enum { FGPE_FP64 = 0, FGPE_FP32 = 1 };
@@ -206,13 +209,41 @@ int fgpe_batch_observables(fgpe_batch_t *b, double *out, int with_conv);
  * for the whole group, each launch walking the tiles of all its instances;
  * the other instances keep their own branches.  The results are those of
  * the single-instance passes up to the NORMC summation order. */
-enum { FGPE_BATCH_BRANCHES = 0, FGPE_BATCH_GROUPED = 1 };
+/* FGPE_BATCH_PERSISTENT: the same instances (any mix of those grid sizes,
+ * per spin and precision) advance by ONE persistent kernel launch per
+ * captured graph of K steps.  Its blocks take work items (column tiles, then
+ * row chunks, of every instance, step after step) from a device ticket
+ * counter; per-instance device counters order a step's row pass after its
+ * column pass and the next step after the NORMC of this one, so instances
+ * of different sizes overlap.  Every device-side wait is bounded
+ * (fgpe_batch_wait_bound); when one runs out the step call returns
+ * FGPE_E_TIMEOUT.  No counterpart in the reference (one instance per
+ * ./cgpe.x process; its loop at cgpe2d.f90:440-531). */
+enum { FGPE_BATCH_BRANCHES = 0, FGPE_BATCH_GROUPED = 1, FGPE_BATCH_PERSISTENT = 2 };
 int fgpe_batch_mode(fgpe_batch_t *b, int mode);
 
+/* Persistent kernel variant (0 .. fgpe_batch_variants()-1) of the batch:
+ * variant >= 0 selects one, -1 keeps the current; *current (may be NULL)
+ * receives the selection.  fgpe_batch_variant_shape writes the variant's
+ * shape[4] = {threads per block, values per row tile, bytes of x per column
+ * tile row, radix plan of the y lines (0: radix 8 first, then 4 or 2;
+ * 1: 4*4 in place of a trailing 8*2; 2: plan 0 reversed)}. */
+int fgpe_batch_variant(fgpe_batch_t *b, int variant, int *current);
+int fgpe_batch_variant_shape(int variant, int *shape);
+int fgpe_batch_variants(void);
+/* Bound on one device-side wait of the persistent kernel (ms of device
+ * time, default 2000).  stall_instance >= 0 is a test hook: that instance's
+ * first row wait then waits for a count no block produces, so the bound
+ * runs out and the step returns FGPE_E_TIMEOUT (-1: none). */
+int fgpe_batch_wait_bound(fgpe_batch_t *b, double wait_ms, int stall_instance);
+
 /* Autotuner: times kernel family per grid-size class, branch width and
- * steps per graph on the batch itself (states saved and restored) and keeps
- * the fastest; cache_path (may be NULL) remembers the choice per batch
- * signature.  fgpe_batch_tuning reports the current width and steps. */
+ * steps per graph with one graph branch per instance, the grouped mode, and
+ * the persistent mode with every kernel variant (threads per block, row and
+ * column tile shapes, radix plan of the y lines), on the batch itself
+ * (states saved and restored) and keeps the fastest; cache_path (may be
+ * NULL) remembers the choice per batch signature.  fgpe_batch_tuning
+ * reports the current width and steps, fgpe_batch_mode-/variant the rest. */
 int fgpe_batch_autotune(fgpe_batch_t *b, int trial_steps, const char *cache_path);
 int fgpe_batch_tuning(const fgpe_batch_t *b, int *width, int *steps_per_graph);
 
