@@ -76,6 +76,12 @@ struct fgpe_s {
     bool has_fast_row = false, has_fast_col[3] = {false, false, false};
     int fast_row_grid = 0, fast_col_grid[3] = {0, 0, 0};
     bool col_wide[3] = {false, false, false};   // column pass uses the wide tiles
+    // column passes that transform forward and back in one launch (q2D y,
+    // 3D z) on the radix-16 plan (cplan pv 3) with its own position map
+    bool col_r16[3] = {false, false, false};
+    int col_r16_grid[3] = {0, 0, 0};
+    int* pmap16 = nullptr;
+    const int* fline16[3] = {nullptr, nullptr, nullptr};
     // row pass with one warp per x row (k_row_warp), where a row fits 16 KB
     bool has_warp_row = false, warp_row = false;
     int warp_row_grid = 0;
@@ -250,6 +256,28 @@ template <typename T, int MS, int N> int setup_fast_col(fgpe_t* h, int n_other, 
     return grid_for(k_col_fast<T, MS, N, col_tx<T>(), col_th<T, MS, N>()>, col_th<T, MS, N>(), col_smem<T, MS, N>(),
                     (h->p.nx / col_tx<T>()) * n_other);
 }
+// Radix-16 plan for the column passes that transform forward and back in one
+// launch, on lengths where it saves a radix pass (128, 256, 384); build knob
+// FGPE_COL_R16 (0: every column pass on the handle's plan).
+#ifndef FGPE_COL_R16
+#define FGPE_COL_R16 1
+#endif
+constexpr bool r16_len(int n) { return FGPE_COL_R16 && cplan(n, 3).r[0] == 16; }
+// Grid of the radix-16 form of the column kernel with the same tiles as
+// setup_fast_col chose (0: not available).
+template <typename T, int MS, int N> int setup_fast_col_r16(fgpe_t* h, int n_other, bool wide) {
+    if constexpr (r16_len(N)) {
+        if constexpr (wide_ok<T, MS, N>()) {
+            if (wide)
+                return grid_for(k_col_fast<T, MS, N, col_txw<T>(), col_th_w<T, MS, N>(), FGPE_COL_NBUF_W, 3>,
+                                col_th_w<T, MS, N>(), col_smem_w<T, MS, N>(), (h->p.nx / col_txw<T>()) * n_other);
+        }
+        if (!wide)
+            return grid_for(k_col_fast<T, MS, N, col_tx<T>(), col_th<T, MS, N>(), FGPE_COL_NBUF, 3>, col_th<T, MS, N>(),
+                            col_smem<T, MS, N>(), (h->p.nx / col_tx<T>()) * n_other);
+    }
+    return 0;
+}
 // Warp-row kernel: rows of MS lines up to 16 KB (FP64 spin-1 to 256 points,
 // spin-2 to 128; FP32 spin-1 to 512, spin-2 to 256); warps per block so that
 // two blocks of NBUF rows per warp fit the shared memory.
@@ -306,7 +334,23 @@ template <typename T, int MS, int N> void run_warp_row(fgpe_t* h, const RowArgs&
                    (size_t)W * FGPE_WROW_NBUF * wrow_tile<T, MS, N>(), a);
     }
 }
-template <typename T, int MS, int N> void run_fast_col(fgpe_t* h, int axis, const ColArgs& a) {
+template <typename T, int MS, int N> void run_fast_col(fgpe_t* h, int axis, const ColArgs& a0) {
+    ColArgs a = a0;
+    if constexpr (r16_len(N)) {
+        if (h->col_r16[axis] && (a.flags & COL_FWD) && (a.flags & COL_INV)) {
+            a.fline = h->fline16[axis];
+            if constexpr (wide_ok<T, MS, N>()) {
+                if (h->col_wide[axis]) {
+                    launch_pdl(h, k_col_fast<T, MS, N, col_txw<T>(), col_th_w<T, MS, N>(), FGPE_COL_NBUF_W, 3>,
+                               h->col_r16_grid[axis], col_th_w<T, MS, N>(), col_smem_w<T, MS, N>(), a);
+                    return;
+                }
+            }
+            launch_pdl(h, k_col_fast<T, MS, N, col_tx<T>(), col_th<T, MS, N>(), FGPE_COL_NBUF, 3>, h->col_r16_grid[axis],
+                       col_th<T, MS, N>(), col_smem<T, MS, N>(), a);
+            return;
+        }
+    }
     if constexpr (wide_ok<T, MS, N>()) {
         if (h->col_wide[axis]) {
             launch_pdl(h, k_col_fast<T, MS, N, col_txw<T>(), col_th_w<T, MS, N>(), FGPE_COL_NBUF_W>, h->fast_col_grid[axis],
@@ -391,6 +435,7 @@ void launch_col(fgpe_t* h, int axis, int flags) {
     a.flags = flags;
     a.n_other = h->p.dim == 2 ? 1 : (axis == 1 ? h->p.nz : h->p.ny);
     a.axis = axis;
+    a.fline = axis == 1 ? h->sc.fy : h->sc.fz;
     ProfScope ps(h, axis);
     if (h->fast_col[axis]) {
 #define RUNC(NN) run_fast_col<T, MS, NN>(h, axis, a)
@@ -896,6 +941,28 @@ int fgpe_create(const fgpe_params* pin, fgpe_t** out) {
         FAST_SWITCH(ns[a], SETC)
 #undef SETC
         if (g > 0) { h->fast_col[a] = h->has_fast_col[a] = true; h->fast_col_grid[a] = g; h->col_wide[a] = wide; }
+        // the pass that carries KE and SOC (q2D y, 3D z) transforms forward
+        // and back in one launch: its lines may take the radix-16 plan
+        const bool fused = (p.dim == 2 && a == 1) || (p.dim == 3 && a == 2);
+        if (g > 0 && fused && r16_len(ns[a])) {
+            int g16 = 0;
+#define SETC16(NN) g16 = h->fp32 ? (ms == 3 ? setup_fast_col_r16<float, 3, NN>(h, nob, wide) : setup_fast_col_r16<float, 5, NN>(h, nob, wide)) \
+                                 : (ms == 3 ? setup_fast_col_r16<double, 3, NN>(h, nob, wide) : setup_fast_col_r16<double, 5, NN>(h, nob, wide))
+            FAST_SWITCH(ns[a], SETC16)
+#undef SETC16
+            if (g16 > 0) {
+                const CPlan cp = cplan(ns[a], 3);
+                FftPlan pl;
+                pl.n = ns[a]; pl.nf = cp.nf;
+                for (int f = 0; f < cp.nf; ++f) pl.r[f] = cp.r[f];
+                const std::vector<int> f = position_map(pl);
+                if (!h->pmap16) CK(cudaMalloc(&h->pmap16, 2 * 512 * sizeof(int)));
+                CK(cudaMemcpy(h->pmap16 + (a - 1) * 512, f.data(), f.size() * sizeof(int), cudaMemcpyHostToDevice));
+                h->fline16[a] = h->pmap16 + (a - 1) * 512;
+                h->col_r16[a] = true;
+                h->col_r16_grid[a] = g16;
+            }
+        }
     }
     cudaGetLastError();   // clear any attribute/occupancy probe error
     h->obsl.grid = dim3((unsigned)((h->npts + 255) / 256));
@@ -945,7 +1012,7 @@ int fgpe_destroy(fgpe_t* h) {
     if (h->bulk) cudaGraphExecDestroy(h->bulk);
     cudaFree(h->S); cudaFree(h->psi); cudaFree(h->prev); cudaFree(h->stage);
     cudaFree(h->dtab); cudaFree(h->ctab); cudaFree(h->part); cudaFree(h->info);
-    cudaFree(h->counters); cudaFree(h->pmap);
+    cudaFree(h->counters); cudaFree(h->pmap); cudaFree(h->pmap16);
     if (h->h_small) cudaFreeHost(h->h_small);
     for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
     if (h->own_stream && h->st) cudaStreamDestroy(h->st);

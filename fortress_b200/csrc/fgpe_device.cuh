@@ -140,6 +140,43 @@ template <typename T, bool INV> struct Dft<T, INV, 8> {
         for (int k = 0; k < 4; ++k) { v[2 * k] = a[k]; v[2 * k + 1] = b[k]; }
     }
 };
+// 16 points as 4 x 4: x[n1 + 4 n2] -> 4-point DFTs over n2, twiddles
+// W16^(n1 k2), 4-point DFTs over n1 -> X[4 k1 + k2] (natural order out).
+template <typename T, bool INV> struct Dft<T, INV, 16> {
+    static __device__ __forceinline__ cx<T> rot(cx<T> a, T c, T s) {   // a * (c + i s)
+        return mk<T>(a.x * c - a.y * s, a.x * s + a.y * c);
+    }
+    static __device__ __forceinline__ void run(cx<T>* v) {
+        const T sg = INV ? (T)1 : (T)-1;
+        const T c1 = (T)0.92387953251128675612818318939678828682;   // cos(pi/8)
+        const T s1 = (T)0.38268343236508977172845998403039886676;   // sin(pi/8)
+        const T h = (T)0.70710678118654752440084436210484903928;    // cos(pi/4)
+        cx<T> y[4][4];
+#pragma unroll
+        for (int n1 = 0; n1 < 4; ++n1) {
+#pragma unroll
+            for (int n2 = 0; n2 < 4; ++n2) y[n1][n2] = v[n1 + 4 * n2];
+            Dft<T, INV, 4>::run(y[n1]);
+        }
+        // W16^m = cos(m pi/8) + i sg sin(m pi/8) for m = n1 k2
+        y[1][1] = rot(y[1][1], c1, sg * s1);
+        y[1][2] = rot(y[1][2], h, sg * h);
+        y[1][3] = rot(y[1][3], s1, sg * c1);
+        y[2][1] = rot(y[2][1], h, sg * h);
+        y[2][2] = cmuli(y[2][2], INV ? 1 : -1);
+        y[2][3] = rot(y[2][3], -h, sg * h);
+        y[3][1] = rot(y[3][1], s1, sg * c1);
+        y[3][2] = rot(y[3][2], -h, sg * h);
+        y[3][3] = rot(y[3][3], -c1, -sg * s1);
+#pragma unroll
+        for (int k2 = 0; k2 < 4; ++k2) {
+            cx<T> z[4] = {y[0][k2], y[1][k2], y[2][k2], y[3][k2]};
+            Dft<T, INV, 4>::run(z);
+#pragma unroll
+            for (int k1 = 0; k1 < 4; ++k1) v[4 * k1 + k2] = z[k1];
+        }
+    }
+};
 template <typename T, bool INV> struct Dft<T, INV, 3> {
     static __device__ __forceinline__ void run(cx<T>* v) {
         const T s = (T)0.86602540378443864676372317075293618347 * (INV ? 1 : -1);

@@ -24,8 +24,21 @@ struct CPlan {
 // pv = 2: the radices of plan 0 in reverse order (small radices on the
 // longest stride).  Only transforms whose spectra stay inside one kernel
 // (the y lines of the persistent batch kernel) use pv != 0.
+// pv = 3: a radix-16 pass first where it saves a pass: 2^7 -> 16*8,
+// 2^8 -> 16*16 (128, 256, 384 = 16*8*3); other lengths as plan 0.  Used by
+// the column passes that transform forward and back in one launch (the q2D
+// y pass, the 3D z pass), whose spectra never leave the kernel.
 constexpr CPlan cplan(int n, int pv = 0) {
     CPlan p{0, {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0}};
+    if (pv == 3) {
+        int e = 0, m = n;
+        while (m % 2 == 0) { m /= 2; ++e; }
+        if (e == 7 || e == 8) {
+            p.r[p.nf++] = 16;
+            p.r[p.nf++] = e == 7 ? 8 : 16;
+            n = m;
+        }
+    }
     while (n % 8 == 0) { p.r[p.nf++] = 8; n /= 8; }
     if (n % 4 == 0) { p.r[p.nf++] = 4; n /= 4; }
     if (n % 2 == 0) {
@@ -410,7 +423,9 @@ __global__ void __launch_bounds__(WPB * 32, 2) k_row_warp(StepConst c, RowArgs a
 // --------------------------------------------------------- column kernel
 // Tiles of TX adjacent x positions, full lines of N along the transformed
 // axis; persistent over (x-tile, other) pairs.
-template <typename T, int MS, int N, int TX, int TH, int NBUF = FGPE_COL_NBUF>
+// PV: radix plan of the lines (cplan); a plan other than the handle's needs
+// a pass that transforms forward and back, with a.fline its position map.
+template <typename T, int MS, int N, int TX, int TH, int NBUF = FGPE_COL_NBUF, int PV = 0>
 __global__ void __launch_bounds__(TH, FGPE_COL_MINB) k_col_fast(StepConst c, ColArgs a) {
     asm volatile("griddepcontrol.wait;\n" ::: "memory");
     using CT = ColTile<N, TX>;
@@ -487,7 +502,7 @@ __global__ void __launch_bounds__(TH, FGPE_COL_MINB) k_col_fast(StepConst c, Col
             }
             __syncthreads();
         }
-        if (a.flags & COL_FWD) ct_fft<T, false, N, MS * TX, TH, CT>(cur, tw);
+        if (a.flags & COL_FWD) ct_fft<T, false, N, MS * TX, TH, CT, 0, 0, PV>(cur, tw);
         if (a.flags & COL_KOP) {
             // z lines: (kx, ky) is fixed along each line of the tile, so the
             // SO-coupling exponential is one MS x MS matrix per tile column,
@@ -516,7 +531,7 @@ __global__ void __launch_bounds__(TH, FGPE_COL_MINB) k_col_fast(StepConst c, Col
                 const int ix = c.fx[x0 + t];
                 // y lines: ky at the line position; z lines: ky at the tile's y
                 int iy, iz;
-                if (a.axis == 1) { iy = c.fy[e]; iz = 0; } else { iy = c.fy[oth]; iz = c.fz[e]; }
+                if (a.axis == 1) { iy = a.fline[e]; iz = 0; } else { iy = c.fy[oth]; iz = a.fline[e]; }
                 cx<T> v[MS];
 #pragma unroll
                 for (int m = 0; m < MS; ++m) v[m] = cur[(m * LPN + e + (e >> 3)) * TX + t];
@@ -554,7 +569,7 @@ __global__ void __launch_bounds__(TH, FGPE_COL_MINB) k_col_fast(StepConst c, Col
             }
             __syncthreads();
         }
-        if (a.flags & COL_INV) ct_fft<T, true, N, MS * TX, TH, CT>(cur, tw);
+        if (a.flags & COL_INV) ct_fft<T, true, N, MS * TX, TH, CT, 0, 0, PV>(cur, tw);
         for (int idx = threadIdx.x; idx < MS * N * TX; idx += TH) {
             const int t = idx % TX, q = idx / TX, e = q % N, m = q / N;
             S[(size_t)m * np + off + (size_t)e * a.axis_stride + t] = cur[(m * LPN + e + (e >> 3)) * TX + t];

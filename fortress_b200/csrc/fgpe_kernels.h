@@ -49,6 +49,7 @@ struct ColArgs {
     int n, tx, flags;
     int n_other;       // number of positions along the third axis (1 in 2D)
     int axis;          // transformed axis: 1 (y) or 2 (z)
+    const int* fline;  // position -> frequency map of the transformed axis in the pass's radix plan
 };
 
 // Long 1D lines, N = N1*N2 points, handled as an N2 x N1 array (x = n1 + N1*n2)

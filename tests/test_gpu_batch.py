@@ -155,7 +155,10 @@ def test_grouped_batch_matches_individual(F):
         s.step(12)
     obs = b.observables()
     for i, p in enumerate(insts):
-        tol = 1e-13 if p["precision"] == "fp64" else 2e-6
+        # FP32: a single handle's y pass on 128-point lines takes the radix-16
+        # plan, the grouped kernels radix 8*8*2: different FP32 rounding of the
+        # transforms, 2.7e-6 of the largest value after the 12 real-time steps
+        tol = 1e-13 if p["precision"] == "fp64" else 5e-6
         sa, sb = b[i].state(), singles[i].state()
         assert np.abs(sa - sb).max() <= tol * np.abs(sb).max(), (i, float(np.abs(sa - sb).max()))
         # reductions are FP64 in both precisions, of states that agree to tol

@@ -50,12 +50,11 @@ def test_persistent_matches_individual(F, variant):
     for s in singles:
         s.step(12)
     obs = b.observables()
-    # a y radix plan other than the handles' (variant 1) rounds the FP32
-    # transforms differently: 2.4e-6 of the largest value after the 12
-    # real-time spin-2 steps, where the handles' own plan stays under 2e-6
-    y_plan = b.variant_shapes()[variant]["y_plan"]
+    # FP32: the y radix plans differ (a single handle's y pass takes the
+    # radix-16 plan on 128-point lines), so the transforms round differently:
+    # up to 2.7e-6 of the largest value after the 12 real-time spin-2 steps
     for i, p in enumerate(insts):
-        tol = 1e-13 if p["precision"] == "fp64" else (2e-6 if y_plan == 0 else 5e-6)
+        tol = 1e-13 if p["precision"] == "fp64" else 5e-6
         sa, sb = b[i].state(), singles[i].state()
         assert np.abs(sa - sb).max() <= tol * np.abs(sb).max(), (i, float(np.abs(sa - sb).max()))
         rt = 1e-12 if p["precision"] == "fp64" else 1e-6
@@ -112,7 +111,7 @@ def test_persistent_wait_runs_out(F):
     for s in singles:
         s.step(4)
     for i, p in enumerate(insts):
-        tol = 1e-13 if p["precision"] == "fp64" else 2e-6
+        tol = 1e-13 if p["precision"] == "fp64" else 5e-6   # radix plans as above
         sa, sb = b[i].state(), singles[i].state()
         assert np.abs(sa - sb).max() <= tol * np.abs(sb).max(), i
 
