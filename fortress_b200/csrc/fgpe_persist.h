@@ -14,12 +14,13 @@ struct PersistShape {
     int txb;   // bytes of x per column tile row
     int pv;    // radix plan of the y lines (cplan)
 };
-constexpr int kPersistVariants = 4;
+constexpr int kPersistVariants = 5;
 constexpr PersistShape kPersistShapes[kPersistVariants] = {
     {256, 512, 32, 0},    // base shape
     {256, 512, 32, 1},    // radix 4*4 in place of 8*2 on the y lines (128, 384)
     {256, 1024, 32, 0},   // twice the rows per row tile
     {128, 256, 16, 0},    // small blocks: more of them per SM
+    {256, 1024, 32, 3},   // tall row tiles, radix-16 y lines (128, 256, 384)
 };
 
 // Set the variant's shared-memory limit and report its resident blocks per SM

@@ -25,6 +25,7 @@ template <typename T, int MS> cudaError_t persist_prepare(int variant, size_t sm
         case 1: return persist_prepare_v<T, MS, 1>(smem, blocks_per_sm);
         case 2: return persist_prepare_v<T, MS, 2>(smem, blocks_per_sm);
         case 3: return persist_prepare_v<T, MS, 3>(smem, blocks_per_sm);
+        case 4: return persist_prepare_v<T, MS, 4>(smem, blocks_per_sm);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -34,7 +35,7 @@ cudaError_t persist_launch(int variant, const PersistArgs& a, int grid, size_t s
     switch (variant) {
 #define PL(V) \
         case V: persist_kernel<T, MS, V>()<<<grid, kPersistShapes[V].th, smem, st>>>(a); break;
-        PL(0) PL(1) PL(2) PL(3)
+        PL(0) PL(1) PL(2) PL(3) PL(4)
 #undef PL
         default: return cudaErrorInvalidValue;
     }

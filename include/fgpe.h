@@ -227,7 +227,8 @@ int fgpe_batch_mode(fgpe_batch_t *b, int mode);
  * receives the selection.  fgpe_batch_variant_shape writes the variant's
  * shape[4] = {threads per block, values per row tile, bytes of x per column
  * tile row, radix plan of the y lines (0: radix 8 first, then 4 or 2;
- * 1: 4*4 in place of a trailing 8*2; 2: plan 0 reversed)}. */
+ * 1: 4*4 in place of a trailing 8*2; 2: plan 0 reversed; 3: a radix-16
+ * pass first where it saves a pass, 128 = 16*8, 256 = 16*16, 384 = 16*8*3)}. */
 int fgpe_batch_variant(fgpe_batch_t *b, int variant, int *current);
 int fgpe_batch_variant_shape(int variant, int *shape);
 int fgpe_batch_variants(void);

@@ -31,7 +31,7 @@ def _start(F, insts, b, seed=20):
     return singles
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
 def test_persistent_matches_individual(F, variant):
     """Spin-1 FP64 instances of 128^2, 512^2 and 384x256 (imaginary and real
     time) share one launch, the spin-2 FP32 192x128 pair another, and a 96x80
