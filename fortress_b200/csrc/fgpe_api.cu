@@ -334,10 +334,10 @@ template <typename T, int MS, int N> void run_warp_row(fgpe_t* h, const RowArgs&
                    (size_t)W * FGPE_WROW_NBUF * wrow_tile<T, MS, N>(), a);
     }
 }
-template <typename T, int MS, int N> void run_fast_col(fgpe_t* h, int axis, const ColArgs& a0) {
+template <typename T, int MS, int N> void run_fast_col(fgpe_t* h, int axis, const ColArgs& a0, bool r16) {
     ColArgs a = a0;
     if constexpr (r16_len(N)) {
-        if (h->col_r16[axis] && (a.flags & COL_FWD) && (a.flags & COL_INV)) {
+        if (r16) {
             a.fline = h->fline16[axis];
             if constexpr (wide_ok<T, MS, N>()) {
                 if (h->col_wide[axis]) {
@@ -436,9 +436,16 @@ void launch_col(fgpe_t* h, int axis, int flags) {
     a.n_other = h->p.dim == 2 ? 1 : (axis == 1 ? h->p.nz : h->p.ny);
     a.axis = axis;
     a.fline = axis == 1 ? h->sc.fy : h->sc.fz;
+    // radix-16 lines: a pass that transforms forward and back (q2D y, 3D z),
+    // or the y passes of a 3D step when all its column passes run the
+    // size-specialised kernels (the y spectra then use that plan throughout
+    // the step: the z pass reads ky through fother)
+    const bool y16 = h->p.dim == 3 && (flags & COL_STEP) && h->col_r16[1] && h->fast_col[1] && h->fast_col[2];
+    a.fother = y16 ? h->fline16[1] : h->sc.fy;
+    const bool r16 = h->col_r16[axis] && ((axis == 1 && y16) || ((flags & COL_FWD) && (flags & COL_INV)));
     ProfScope ps(h, axis);
     if (h->fast_col[axis]) {
-#define RUNC(NN) run_fast_col<T, MS, NN>(h, axis, a)
+#define RUNC(NN) run_fast_col<T, MS, NN>(h, axis, a, r16)
         FAST_SWITCH(a.n, RUNC)
 #undef RUNC
         h->launches++;
@@ -942,8 +949,9 @@ int fgpe_create(const fgpe_params* pin, fgpe_t** out) {
 #undef SETC
         if (g > 0) { h->fast_col[a] = h->has_fast_col[a] = true; h->fast_col_grid[a] = g; h->col_wide[a] = wide; }
         // the pass that carries KE and SOC (q2D y, 3D z) transforms forward
-        // and back in one launch: its lines may take the radix-16 plan
-        const bool fused = (p.dim == 2 && a == 1) || (p.dim == 3 && a == 2);
+        // and back in one launch, and the 3D y spectra live only between the
+        // step's two y passes: these lines may take the radix-16 plan
+        const bool fused = (p.dim == 2 && a == 1) || p.dim == 3;
         if (g > 0 && fused && r16_len(ns[a])) {
             int g16 = 0;
 #define SETC16(NN) g16 = h->fp32 ? (ms == 3 ? setup_fast_col_r16<float, 3, NN>(h, nob, wide) : setup_fast_col_r16<float, 5, NN>(h, nob, wide)) \
@@ -1165,11 +1173,11 @@ int fgpe_step_ex(fgpe_t* h, int nsteps, int flags) {
             return;
         }
         if (h->p.dim == 2) {
-            DISPATCH(h, launch_col, h, 1, COL_SCALE | COL_FWD | COL_KOP | COL_INV);
+            DISPATCH(h, launch_col, h, 1, COL_SCALE | COL_FWD | COL_KOP | COL_INV | COL_STEP);
         } else {
-            DISPATCH(h, launch_col, h, 1, COL_SCALE | COL_FWD);
-            DISPATCH(h, launch_col, h, 2, COL_FWD | COL_KOP | COL_INV);
-            DISPATCH(h, launch_col, h, 1, COL_INV);
+            DISPATCH(h, launch_col, h, 1, COL_SCALE | COL_FWD | COL_STEP);
+            DISPATCH(h, launch_col, h, 2, COL_FWD | COL_KOP | COL_INV | COL_STEP);
+            DISPATCH(h, launch_col, h, 1, COL_INV | COL_STEP);
         }
         DISPATCH(h, launch_row, h, ROW_FULL, sn);
     };

@@ -515,7 +515,7 @@ __global__ void __launch_bounds__(TH, FGPE_COL_MINB) k_col_fast(StepConst c, Col
                     cx<T> u[MS];
 #pragma unroll
                     for (int m = 0; m < MS; ++m) u[m] = mk<T>(m == j ? (T)1 : (T)0, (T)0);
-                    const int ixt = c.fx[x0 + t], iyt = c.fy[oth];
+                    const int ixt = c.fx[x0 + t], iyt = a.fother[oth];
                     apply_soc<T, MS>(c, c.kx[ixt], c.ky[iyt], u);
                     // the kx, ky part of KE, exp(-i CDT (kx^2 + ky^2)), is a
                     // scalar along the line: folded into the matrix
@@ -531,7 +531,7 @@ __global__ void __launch_bounds__(TH, FGPE_COL_MINB) k_col_fast(StepConst c, Col
                 const int ix = c.fx[x0 + t];
                 // y lines: ky at the line position; z lines: ky at the tile's y
                 int iy, iz;
-                if (a.axis == 1) { iy = a.fline[e]; iz = 0; } else { iy = c.fy[oth]; iz = a.fline[e]; }
+                if (a.axis == 1) { iy = a.fline[e]; iz = 0; } else { iy = a.fother[oth]; iz = a.fline[e]; }
                 cx<T> v[MS];
 #pragma unroll
                 for (int m = 0; m < MS; ++m) v[m] = cur[(m * LPN + e + (e >> 3)) * TX + t];

@@ -24,7 +24,10 @@ enum { ROW_FULL = 0, ROW_FWD = 1, ROW_INV = 2 };
 // Column-pass work: COL_KE and COL_SOC act in k-space between the forward
 // and inverse transforms of the pass (KE before SOC, cgpe3d.f90:452-454).
 // Every step applies both in one pass (2D: the y pass; 3D: the z pass).
-enum { COL_SCALE = 1, COL_FWD = 2, COL_KE = 4, COL_INV = 8, COL_SOC = 16, COL_KOP = COL_KE | COL_SOC };
+// COL_STEP marks the passes of a split step: between the forward and inverse y
+// passes of a 3D step the y spectra never leave the step, so those passes may
+// use a radix plan of their own (with ColArgs::fline / fother its maps).
+enum { COL_SCALE = 1, COL_FWD = 2, COL_KE = 4, COL_INV = 8, COL_SOC = 16, COL_KOP = COL_KE | COL_SOC, COL_STEP = 32 };
 enum { OBS_FULL = 0, OBS_NORMS = 1, OBS_NORMALIZE = 2 };
 enum { OP_KE = 1, OP_SOC = 2, OP_SE = 3, OP_SP = 4, OP_SCALE = 5 };
 
@@ -50,6 +53,7 @@ struct ColArgs {
     int n_other;       // number of positions along the third axis (1 in 2D)
     int axis;          // transformed axis: 1 (y) or 2 (z)
     const int* fline;  // position -> frequency map of the transformed axis in the pass's radix plan
+    const int* fother; // z lines: position -> frequency map of y, in the plan of the step's y passes
 };
 
 // Long 1D lines, N = N1*N2 points, handled as an N2 x N1 array (x = n1 + N1*n2)
