@@ -1917,6 +1917,9 @@ int capture_persistent(fgpe_batch_t* b, int nsteps) {
     drop_graph(b);
     int r = build_psets(b);
     if (r) return r;
+    for (const PersistSet& p : b->psets)   // tickets are 32-bit: items per launch stay below 2^31
+        if ((long long)(p.ncol + p.nrow) * nsteps >= (1LL << 31))
+            return bfail(b, FGPE_E_ARG, "persistent batch: too many work items per launch (lower steps_per_graph)");
     for (fgpe_t* h : b->inst) {
         if (!h->has_state) return bfail(b, FGPE_E_STATE, "batch instance without a state");
         if (h->p.dim >= 2 && !h->S_valid) {
